@@ -1,0 +1,316 @@
+/*
+ * libngs -- B200 (sm_100a) kernels for the sparse screened-Poisson
+ * reconstruction path of neural-galerkin ("jspsr").
+ *
+ * C ABI: plain pointers and sizes, no framework types.  Unless stated
+ * otherwise every pointer is DEVICE memory, every call is asynchronous on the
+ * given stream, nothing is allocated inside the library, and the return value
+ * is an ngs_status.  Where the reference's op returned a freshly allocated
+ * tensor, the caller passes the output buffer (and, where needed, a scratch
+ * workspace whose size a *_workspace_bytes() query reports).
+ *
+ * Citations "ref: file:line" name the reference interface an entry point
+ * replaces (paths inside huangjh-pub/neural-galerkin).
+ */
+#ifndef NGS_H_
+#define NGS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* ngs_stream;   /* == cudaStream_t */
+
+typedef enum {
+  NGS_OK = 0,
+  NGS_ERR_INVALID_ARG = 1,
+  NGS_ERR_OOM = 2,               /* caller-provided buffer / workspace too small */
+  NGS_ERR_HASH_INSERT = 3,       /* hash table full or probe bound exceeded */
+  NGS_ERR_NOT_CONVERGED = 4,     /* iterative solve hit max_iter above tolerance */
+  NGS_ERR_TOPOLOGY = 5,          /* dual-grid corner accumulation overflow */
+  NGS_ERR_CUDA = 6,              /* CUDA runtime error: see ngs_last_cuda_error() */
+  NGS_ERR_TIMEOUT = 7            /* a bounded device-side wait gave up */
+} ngs_status;
+
+const char* ngs_status_string(int status);
+const char* ngs_last_cuda_error(void);
+int ngs_version(void);
+
+/* ======================================================================= hashing
+ * ref: csrc/common/hashmap_cuda.cu:247-305 (hash_cuda), :204-235,307-339
+ * (kernel_hash_cuda), :341-379 (build_hash_table), :381-398 (hash_table_query);
+ * Python binding jspsr/ext.py:14-84 (CuckooHashTable).
+ * Keys: FNV-1a-64 over (uint32) coordinates folded to 60 bits, bit-identical
+ * to the reference.  The table is an open-addressing table of 16-byte
+ * {key, value} slots probed by 8-lane groups (one 128-byte bucket per probe);
+ * query results (value + 1, 0 = absent) are identical to the reference's
+ * cuckoo table, the slot layout is not (the reference's is randomised).      */
+
+typedef struct ngs_hash_table {
+  void* slots;          /* nslots x {uint64 key, int64 value}, 16-byte aligned */
+  int64_t nslots;       /* power of two, >= 8 */
+  int64_t inserted;     /* number of keys inserted (HashLookupData.inserted_size) */
+} ngs_hash_table;
+
+/* hash_cuda: coords int32 or int64 [n, dim], dim in {2,3,4} -> out int64[n] */
+int ngs_hash_coords(const void* coords, int coords_int64, int64_t n, int dim, int64_t* out, ngs_stream s);
+/* kernel_hash_cuda: coords [n, 3|4], offsets int32 [k, 3] -> out int64 [k, n] (k-major) */
+int ngs_kernel_hash(const void* coords, int coords_int64, int64_t n, int dim, const int32_t* offsets,
+                    int64_t k, int64_t* out, ngs_stream s);
+/* Slot count the builder needs for n keys (load <= 1/2, or <= 1/4 when enlarge). */
+int64_t ngs_hash_table_slots(int64_t n, int enlarge);
+/* build_hash_table: vals == NULL means value = row index.  table->slots must hold
+ * table->nslots slots; status_dev (int, device) receives NGS_ERR_HASH_INSERT on failure.
+ * A repeated key keeps the smallest value. */
+int ngs_hash_table_build(ngs_hash_table* table, const int64_t* keys, const int64_t* vals, int64_t n,
+                         int* status_dev, ngs_stream s);
+/* hash_table_query: out[i] = value + 1 where keys[i] is present, else 0 */
+int ngs_hash_table_query(const ngs_hash_table* table, const int64_t* keys, int64_t m, int64_t* out,
+                         ngs_stream s);
+/* Convenience: out[i] = row of coords[i] (int32 [m,3]) or -1, through FNV keys. */
+int ngs_hash_table_query_coords(const ngs_hash_table* table, const int32_t* coords, int64_t m,
+                                int64_t* out, ngs_stream s);
+
+/* ======================================================================= scans */
+size_t ngs_scan_workspace_bytes(int64_t n);
+/* Exclusive prefix sum of int64 values; *total_dev receives the sum.
+ * ref: the torch::cumsum calls of csrc/sparse_op/sparse_product.cu:222-223,
+ * csrc/marching_cubes/dual_mc.cu:162 and jspsr/core/solver.py:41-48. */
+int ngs_exclusive_scan_i64(const int64_t* in, int64_t n, int64_t* out, int64_t* total_dev, void* ws,
+                           size_t ws_bytes, ngs_stream s);
+int ngs_exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* total_dev, void* ws,
+                           size_t ws_bytes, ngs_stream s);
+
+/* ======================================================================= voxel index (rank bitmap)
+ * Replaces torch.unique(dim=0) + one CuckooHashTable per level
+ * (ref: jspsr/core/_hash_backend.py:358-378,414-467, jspsr/core/ops.py:103-127).
+ * A level's cells live on a lattice of pitch `stride`; the grid holds one bit
+ * per cell of its box plus per-word prefix counts, so the row of a voxel is
+ * its rank in lexicographic (x, y, z) order.                                  */
+
+typedef struct ngs_grid {
+  int32_t origin[3];    /* min corner of the box, finest-voxel units, multiple of stride */
+  int32_t dims[3];      /* box size in cells */
+  int32_t stride;       /* lattice pitch (power of two) */
+  int32_t log2_stride;
+  int32_t zwords;       /* 64-bit words per (x, y) row: ceil(dims[2] / 64) */
+  int32_t pad_;
+  int64_t nwords;       /* dims[0] * dims[1] * zwords */
+  void* words;          /* nwords x 16 bytes {uint32 rank, uint32 pad, uint64 bits}, zeroed before marking */
+} ngs_grid;
+
+/* min/max of a float [n,3] array -> bbox_dev float[6] = (min xyz, max xyz) */
+int ngs_points_bbox(const float* xyz, int64_t n, float* bbox_dev, ngs_stream s);
+/* Mark the 8 trilinear corner cells of every point with level <= max_level
+ * (levels == NULL: all points). ref: _hash_backend.py:457-462,469-510 */
+int ngs_grid_mark_points(ngs_grid g, const float* xyz, int64_t n, float inv_vs, const int32_t* levels,
+                         int max_level, ngs_stream s);
+/* Mark coords[i] + offsets[j] * offset_scale for every i, j (offsets int32 [n_off, 3]; NULL = origin). */
+int ngs_grid_mark_coords(ngs_grid g, const int32_t* coords, int64_t n, const int32_t* offsets, int n_off,
+                         int offset_scale, ngs_stream s);
+size_t ngs_grid_workspace_bytes(const ngs_grid* g);
+/* Prefix counts over the words; *count_dev (int64) receives the number of cells set. */
+int ngs_grid_finalize(ngs_grid g, void* ws, size_t ws_bytes, int64_t* count_dev, ngs_stream s);
+/* Sorted coordinates of the set cells: coords int32 [count, 3]. */
+int ngs_grid_emit_coords(ngs_grid g, int32_t* coords, ngs_stream s);
+/* rows[i] = row of coords[i] (int32 [n,3]) or -1. */
+int ngs_grid_lookup(ngs_grid g, const int32_t* coords, int64_t n, int64_t* rows, ngs_stream s);
+
+/* ======================================================================= density / splatting
+ * ref: jspsr/core/_hash_backend.py:13-28 (compute_density), :332-356 (splat_data),
+ * :414-444 (point levels), jspsr/__init__.py:40-48 (normal splatting).
+ * inv_vs is fp32(1 / fp32(voxel_size)) (the reference's quantisation), vs is the
+ * FP64 voxel size used for the fractional positions.                          */
+int ngs_splat_weights(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, float* wd, ngs_stream s);
+/* density = (sum_k B(.) wd) / 16; level = clamp(-floor(log4(density / min_density)), 0, depth-1);
+ * weight = 1 / density.  Any output pointer may be NULL. */
+int ngs_density_eval(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, const float* wd,
+                     float min_density, int depth, float* density, int32_t* levels, float* weight, ngs_stream s);
+/* out[row] += trilinear weight * data[p] * scale for points with levels[p] == level
+ * (levels == NULL: all points); data is float [n, dim] or NULL (= 1). */
+int ngs_splat_data(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, const float* data, int dim,
+                   const float* point_scale, const int32_t* levels, int level, float scale, float* out, ngs_stream s);
+
+/* ======================================================================= basis at points
+ * Screening data / evaluate_interpolated support (ref: jspsr/core/reconstructor.py:110-120,
+ * jspsr/core/hashtree.py:157-192).  For every point, its 27 neighbour voxels
+ * (lexicographic k in [-1,1]^3): rows int32 [n, 27] (-1 absent), phi float [n, 27]. */
+int ngs_point_basis(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, int32_t* rows, float* phi,
+                    ngs_stream s);
+/* out[p] (+)= sum_k phi[p,k] * x[rows[p,k]]  (accumulate != 0: add to out) */
+int ngs_point_field(const int32_t* rows, const float* phi, int64_t n, const float* x, float* out, int accumulate,
+                    ngs_stream s);
+/* Field value (grad == 0) or gradient (grad != 0, out float [n,3]) of sum_k B(.) x_k at arbitrary
+ * positions, accumulated into out. ref: jspsr/core/hashtree.py:157-192 */
+int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv_vs, double vs, const float* x, int grad,
+                   float* out, ngs_stream s);
+/* sum_p w[p] * v[p] and sum_p w[p] into sums_dev double[2] (mean-chi level set). */
+int ngs_weighted_sum(const float* v, const float* w, int64_t n, double* sums_dev, ngs_stream s);
+
+/* ======================================================================= Galerkin assembly
+ * ref: jspsr/core/reconstructor.py:122-189, jspsr/bases/bezier_tensor.py:75-121,
+ * csrc/sparse_op/sparse_product.cu:100-137 (screening product).
+ * Same-level matrix A_d: CSR over the 5x5x5 stencil of present voxels, columns
+ * sorted; masks[i] (uint32 x4) flags which of the 125 lexicographic offsets are
+ * present, so the slot of offset o in row i is rowptr[i] + popc(mask below o). */
+int ngs_stencil_count(ngs_grid g, const int32_t* coords, int64_t V, uint32_t* masks, int64_t* counts, ngs_stream s);
+/* cols / stiffness values: stencil125 (double[125]) holds the stiffness of each offset;
+ * diag_slot (int64 [V]) receives the slot of the diagonal entry. */
+int ngs_stencil_fill(ngs_grid g, const int32_t* coords, int64_t V, const uint32_t* masks, const int64_t* rowptr,
+                     const double* stencil125, int32_t* cols, double* vals, int64_t* diag_slot, ngs_stream s);
+/* vals[slot(a, b)] += scale * w[p] * phi[p,a] * phi[p,b] over all point pairs (w NULL = 1). */
+int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n, const float* w, const uint32_t* masks,
+                    const int64_t* rowptr, double scale, double* vals, ngs_stream s);
+/* rhs[row] += scale * sum_p w[p] * phi[p,k]  (screening target term). */
+int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, const float* w, double scale, double* rhs,
+                   ngs_stream s);
+/* Divergence RHS from splatted normals of a data level (ref: reconstructor.py:126-141):
+ * rhs[t] -= int grad B_t . n_data over the pairs of get_neighbours(data, target, 3).
+ * tab_f / tab_g: per-axis 1-D tables (FP64) of the level ratio (see jspsr/bases/tables.py). */
+int ngs_rhs_normals(ngs_grid data_grid, const int32_t* data_coords, int64_t n_data, const float* normals,
+                    ngs_grid tgt_grid, const int32_t* tgt_coords, int64_t n_tgt, const double* tab_c, const double* tab_g,
+                    int tab_len, double* rhs, ngs_stream s);
+/* rhs_fine[i] -= sum_j K(i, j) x_coarse[j] over the range-5 pairs (i fine, j coarse);
+ * tab_c / tab_g are the shifted-integral tables of the ratio, already scaled. ref: reconstructor.py:153-168 */
+int ngs_correction_stiffness(const int32_t* fine_coords, int64_t n_fine, int fine_stride, ngs_grid coarse_grid,
+                             const float* x_coarse, const double* tab_c, const double* tab_g, int tab_len,
+                             double* rhs, ngs_stream s);
+/* rhs[row] -= scale * w[p] * phi[p,k] * field[p]  (screening part of the correction). */
+int ngs_correction_screen(const int32_t* rows, const float* phi, int64_t n, const float* w, const float* field,
+                          double scale, double* rhs, ngs_stream s);
+/* vals32[i] = (float) vals64[i]; inv_diag[i] = 1 / vals64[diag_slot[i]]; b32 = (float) b64 */
+int ngs_finish_system(const double* vals64, int64_t nnz, const int64_t* diag_slot, int64_t V, float* vals32,
+                      float* inv_diag, ngs_stream s);
+
+/* ======================================================================= solver
+ * ref: csrc/sparse_solve/solve_pcg.cu:15-136 (solve_pcg_diag), jspsr/core/solver.py:101-202.
+ * One persistent cooperative kernel per solve: SpMV + both dot products fused,
+ * FP64 reductions in fixed order, bounded grid barriers, convergence decided on
+ * the device.  mode:
+ *   NGS_PCG_REFERENCE  FP32 Jacobi-PCG with the reference's stopping rule
+ *                      (recursive residual <= tol * |b|), optional residual
+ *                      replacement every ceil(sqrt(n)) iterations (res_fix).
+ *   NGS_PCG_MIXED      FP32 SpMV / vectors, FP64 dots, FP64 solution, true FP64
+ *                      residual (vals64, b64) every `replace_every` iterations;
+ *                      stops on the true residual.
+ *   NGS_PCG_FP64       all-FP64 Jacobi-PCG (vals64, b64), device-side loop.        */
+enum { NGS_PCG_REFERENCE = 0, NGS_PCG_MIXED = 1, NGS_PCG_FP64 = 2 };
+
+typedef struct ngs_pcg_system {
+  int64_t n;
+  int64_t nnz;
+  const int64_t* rowptr;     /* [n+1] */
+  const int32_t* cols;       /* [nnz] */
+  const float* vals32;       /* [nnz] (REFERENCE, MIXED) */
+  const double* vals64;      /* [nnz] (MIXED, FP64) */
+  const float* b32;          /* [n]   (REFERENCE) */
+  const double* b64;         /* [n]   (MIXED, FP64) */
+  const float* inv_diag;     /* [n] */
+  float* x32;                /* [n] out (REFERENCE, MIXED: FP32 copy of x) */
+  double* x64;               /* [n] out (MIXED, FP64) */
+} ngs_pcg_system;
+
+typedef struct ngs_pcg_config {
+  int mode;
+  int max_iter;              /* < 0: unbounded (the reference's default) */
+  double tol;                /* relative to |b| */
+  int res_fix;               /* REFERENCE mode: replace every ceil(sqrt(n)) */
+  int replace_every;         /* MIXED mode */
+  int blocks;                /* 0: as many co-resident blocks as fit */
+  double timeout_s;          /* bound of every device-side wait */
+} ngs_pcg_config;
+
+size_t ngs_pcg_workspace_bytes(int64_t n, int mode);
+/* info_dev: int64[4] = {iterations, status, replacements, reserved};
+ * resid_dev: double[2] = {final |r|, |b|}.  Iterations and status are also valid
+ * when the call returns NGS_ERR_NOT_CONVERGED / NGS_ERR_TIMEOUT (read them after sync). */
+int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
+                  int64_t* info_dev, double* resid_dev, ngs_stream s);
+
+/* Plain building blocks for the host-driven FP64 comparator (one launch each). */
+int ngs_spmv64(int64_t n, const int64_t* rowptr, const int32_t* cols, const double* vals, const double* x,
+               double* y, ngs_stream s);
+int ngs_dot64(const double* a, const double* b, int64_t n, double* out_dev, ngs_stream s);
+int ngs_axpby64(int64_t n, double alpha, const double* x, double beta, double* y, ngs_stream s);
+int ngs_mul64(int64_t n, const double* a, const double* b, double* out, ngs_stream s);
+
+/* ======================================================================= reference sparse ops
+ * ref: csrc/sparse_op/sparse_product.cu:52-82 (sparse_meshgrid), :202-258 (screened_multiplication),
+ * :260-322 (screened_multiplication_backward).  a_start / b_start are exclusive prefix sums of the
+ * per-point lengths; val_dim is 1 (float [A]) or 3 (float [A,3]).                              */
+int ngs_sparse_meshgrid(const int64_t* a_start, const int64_t* a_len, const int64_t* b_start, const int64_t* b_len,
+                        const int64_t* ab_start, int64_t n_points, int64_t* a_inds, int64_t* b_inds, ngs_stream s);
+int ngs_screened_multiplication(const ngs_hash_table* pairs, const float* a_val, const float* b_val, int val_dim,
+                                const int64_t* a_inds, const int64_t* b_inds, const int64_t* a_start,
+                                const int64_t* a_len, const int64_t* b_start, const int64_t* b_len,
+                                const float* weight, int64_t n_points, float* res, ngs_stream s);
+int ngs_screened_multiplication_backward(const ngs_hash_table* pairs, const float* a_val, const float* b_val,
+                                         int val_dim, const int64_t* a_inds, const int64_t* b_inds,
+                                         const int64_t* a_start, const int64_t* a_len, const int64_t* b_start,
+                                         const int64_t* b_len, const float* weight, int64_t n_points,
+                                         const float* grad_res, float* grad_a, float* grad_b, float* grad_w,
+                                         ngs_stream s);
+
+/* ref: csrc/integration/ddi.cu:51-76 (ddi_forward), :113-141 (ddi_backward).
+ * src / tgt float [P, 3C] (component-major, axis-minor), rel_pos int64 [P, 3],
+ * ff / dfdf float [C, C, R]; p, q float [P, 3] (overwritten). */
+int ngs_ddi_forward(const float* src, const float* tgt, const int64_t* rel_pos, const float* ff, const float* dfdf,
+                    int64_t n_pairs, int C, int R, float* p, float* q, ngs_stream s);
+int ngs_ddi_backward(const float* src, const float* tgt, const int64_t* rel_pos, const float* ff,
+                     const float* dfdf, const float* grad_p, const float* grad_q, int64_t n_pairs, int C, int R,
+                     float* grad_src, float* grad_tgt, ngs_stream s);
+
+/* ======================================================================= marching cubes
+ * ref: csrc/marching_cubes/primal_mc.cu:170-235 (marching_cubes_sparse), dual_mc.cu:135-189
+ * (dual_marching_cubes_sparse), dual_mc_inds.cu:143-182 (dual_marching_cubes_indices).
+ * Two phases: *_count writes per-cell vertex counts; the caller scans them
+ * (ngs_exclusive_scan_i32) and *_emit writes triangles at the scanned offsets.   */
+int ngs_primal_mc_count(const float* sdf, int64_t n_cubes, int r, int32_t* vcount, ngs_stream s);
+int ngs_primal_mc_emit(const float* base, const float* sdf, int64_t n_cubes, int r, const int64_t* voffset,
+                       float* tris, int32_t* vert_ids, int32_t* src_ids, float* src_w, ngs_stream s);
+/* Dual-cube corner accumulation for one level of primal cells (expanded units):
+ * probes corners / edge / face points of each cell of size `stride` in the
+ * dual-centre index and writes (primal id, depth) into acc int32 [D, 8, 2]; cnt int32 [D]. */
+int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_base, int64_t n_primal, int stride, int depth,
+                             int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s);
+int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_t* primal_base, int64_t n_primal, int stride,
+                             int depth, int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s);
+/* Keep cubes with cnt == 8: keep_dev int32 flags for a scan, then compaction. */
+int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, ngs_stream s);
+int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, const int64_t* keep_offset, int64_t n,
+                        int32_t* acc_out, ngs_stream s);
+int ngs_dual_mc_count(const int32_t* acc, int64_t n_cubes, const float* values, int32_t* vcount, ngs_stream s);
+int ngs_dual_mc_emit(const int32_t* acc, int64_t n_cubes, const float* pos, const float* values,
+                     const int64_t* voffset, float* tris, int32_t* vert_ids, ngs_stream s);
+/* Vertex de-duplication of (vid0, vid1) edge keys (replaces torch.unique(dim=0, return_inverse),
+ * ref: jspsr/core/reconstructor.py:380-383): bucket sort by vid0 over n_primal buckets.
+ * Phase 1 counts per bucket; the caller scans counts into bucket_start; phase 2 scatters and
+ * sorts each bucket, marks first occurrences; the caller scans `first` into vertex ids;
+ * phase 3 writes faces (int64 [n_keys]) and vertex positions. */
+int ngs_vdedup_count(const int32_t* vert_ids, int64_t n_keys, int32_t* bucket_count, ngs_stream s);
+int ngs_vdedup_sort(const int32_t* vert_ids, int64_t n_keys, const int64_t* bucket_start, int64_t n_buckets,
+                    int32_t* bucket_fill, int64_t* sorted_keys, int32_t* first, ngs_stream s);
+int ngs_vdedup_emit(const int32_t* vert_ids, const float* tris, int64_t n_keys, const int64_t* bucket_start,
+                    const int32_t* bucket_count, const int64_t* sorted_keys, const int64_t* vertex_id,
+                    int64_t* faces, float* vertices, ngs_stream s);
+
+/* ======================================================================= multi-level mesh helpers
+ * ref: jspsr/core/reconstructor.py:319-376.  Conformal children: for every parent
+ * (coords at 2*stride) its 8 children at stride, in (0,0,0),(0,0,1),... order;
+ * leaf[i] = 1 when child i has no cell in `finer_parents` (NULL grid words: all leaves). */
+int ngs_conformal_children(const int32_t* parents, int64_t n_parents, int stride, int32_t* children, ngs_stream s);
+int ngs_leaf_flags(const int32_t* cells, int64_t n, ngs_grid finer_parents, int32_t* leaf, ngs_stream s);
+int ngs_compact_coords(const int32_t* coords, const int32_t* keep, const int64_t* keep_offset, int64_t n,
+                       int32_t* out, ngs_stream s);
+/* Expanded primal cells: cell * n_up + (i,j,k) * stride for i,j,k < n_up -> int32 [n * n_up^3, 3];
+ * positions (cell_exp + stride) * evs as float [n * n_up^3, 3] (may be NULL). */
+int ngs_expand_cells(const int32_t* cells, int64_t n, int n_up, int stride, float evs, int32_t* out,
+                     float* pos, ngs_stream s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif  /* NGS_H_ */

@@ -1,0 +1,335 @@
+// Galerkin assembly of the screened-Poisson system on one level
+// (jspsr/core/reconstructor.py:122-189, jspsr/bases/bezier_tensor.py:75-121).
+//
+// Layout: CSR over the lexicographically sorted voxels of the level; the
+// columns of a row are its present neighbours in the 5x5x5 stencil, in
+// lexicographic offset order, hence sorted.  A 128-bit mask per row records
+// which of the 125 offsets are present, so the CSR slot of any (row, offset)
+// pair is rowptr + popc(mask below offset) -- the screening Gram product
+// therefore adds straight into the matrix instead of going through the
+// reference's second hash table keyed by (row, col) pairs.
+#include "ngs_common.cuh"
+
+NGS_DEV int popc_below(const uint4 m, int o) {
+  // number of set bits of the 128-bit mask m strictly below bit o
+  const unsigned w[4] = {m.x, m.y, m.z, m.w};
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int lo = i * 32;
+    if (o >= lo + 32) c += __popc(w[i]);
+    else if (o > lo) c += __popc(w[i] & ((1u << (o - lo)) - 1u));
+  }
+  return c;
+}
+
+// ----------------------------------------------------------------------------- structure
+__global__ void stencil_count_kernel(ngs_grid g, const int32_t* __restrict__ coords, int64_t V,
+                                     uint4* __restrict__ masks, int64_t* __restrict__ counts) {
+  for (int64_t i = ngs_gtid(); i < V; i += ngs_gstride()) {
+    const int cx = coords[i * 3], cy = coords[i * 3 + 1], cz = coords[i * 3 + 2];
+    unsigned w[4] = {0u, 0u, 0u, 0u};
+    int o = 0;
+    for (int dx = -2; dx <= 2; dx++)
+      for (int dy = -2; dy <= 2; dy++)
+        for (int dz = -2; dz <= 2; dz++, o++) {
+          if (grid_row(g, cx + dx * g.stride, cy + dy * g.stride, cz + dz * g.stride) >= 0) w[o >> 5] |= 1u << (o & 31);
+        }
+    masks[i] = make_uint4(w[0], w[1], w[2], w[3]);
+    counts[i] = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+  }
+}
+
+__global__ void stencil_fill_kernel(ngs_grid g, const int32_t* __restrict__ coords, int64_t V,
+                                    const uint4* __restrict__ masks, const int64_t* __restrict__ rowptr,
+                                    const double* __restrict__ stencil, int32_t* __restrict__ cols,
+                                    double* __restrict__ vals, int64_t* __restrict__ diag_slot) {
+  __shared__ double st[125];
+  for (int t = threadIdx.x; t < 125; t += blockDim.x) st[t] = stencil[t];
+  __syncthreads();
+  for (int64_t i = ngs_gtid(); i < V; i += ngs_gstride()) {
+    const int cx = coords[i * 3], cy = coords[i * 3 + 1], cz = coords[i * 3 + 2];
+    const uint4 m = masks[i];
+    const unsigned w[4] = {m.x, m.y, m.z, m.w};
+    int64_t slot = rowptr[i];
+    int o = 0;
+    for (int dx = -2; dx <= 2; dx++)
+      for (int dy = -2; dy <= 2; dy++)
+        for (int dz = -2; dz <= 2; dz++, o++) {
+          if (!((w[o >> 5] >> (o & 31)) & 1u)) continue;
+          cols[slot] = (int32_t)grid_row(g, cx + dx * g.stride, cy + dy * g.stride, cz + dz * g.stride);
+          vals[slot] = st[o];
+          if (o == 62) diag_slot[i] = slot;
+          slot++;
+        }
+  }
+}
+
+extern "C" int ngs_stencil_count(ngs_grid g, const int32_t* coords, int64_t V, uint32_t* masks, int64_t* counts,
+                                 ngs_stream s) {
+  if (!g.words || V < 0 || (V > 0 && (!coords || !masks || !counts))) return NGS_ERR_INVALID_ARG;
+  if (V == 0) return NGS_OK;
+  stencil_count_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(g, coords, V, reinterpret_cast<uint4*>(masks),
+                                                                       counts);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_stencil_fill(ngs_grid g, const int32_t* coords, int64_t V, const uint32_t* masks,
+                                const int64_t* rowptr, const double* stencil125, int32_t* cols, double* vals,
+                                int64_t* diag_slot, ngs_stream s) {
+  if (!g.words || V < 0 || (V > 0 && (!coords || !masks || !rowptr || !stencil125 || !cols || !vals || !diag_slot)))
+    return NGS_ERR_INVALID_ARG;
+  if (V == 0) return NGS_OK;
+  stencil_fill_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(
+      g, coords, V, reinterpret_cast<const uint4*>(masks), rowptr, stencil125, cols, vals, diag_slot);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- screening
+// One warp per point; lane a (< 27) owns the point's neighbour a and adds
+// w * phi_a * phi_b into row a for every present neighbour b.
+__global__ void screen_gram_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi, int64_t n,
+                                   const float* __restrict__ w, const uint4* __restrict__ masks,
+                                   const int64_t* __restrict__ rowptr, double scale, double* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p = ngs_gtid() >> 5; p < n; p += warps) {
+    const int32_t ra = lane < 27 ? rows[p * 27 + lane] : -1;
+    const float pa = lane < 27 ? phi[p * 27 + lane] : 0.f;
+    const double sa = scale * (double)(w ? w[p] : 1.f) * (double)pa;
+    uint4 m = make_uint4(0, 0, 0, 0);
+    int64_t base = 0;
+    if (ra >= 0) {
+      m = masks[ra];
+      base = rowptr[ra];
+    }
+    const int ax = lane / 9, ay = (lane / 3) % 3, az = lane % 3;
+#pragma unroll 3
+    for (int b = 0; b < 27; b++) {
+      const int32_t rb = __shfl_sync(0xffffffffu, ra, b);
+      const float pb = __shfl_sync(0xffffffffu, pa, b);
+      if (ra < 0 || rb < 0) continue;
+      const int bx = b / 9, by = (b / 3) % 3, bz = b % 3;
+      const int o = (bx - ax + 2) * 25 + (by - ay + 2) * 5 + (bz - az + 2);
+      atomicAdd(vals + base + popc_below(m, o), sa * (double)pb);
+    }
+  }
+}
+
+extern "C" int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n, const float* w, const uint32_t* masks,
+                               const int64_t* rowptr, double scale, double* vals, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !phi || !masks || !rowptr || !vals))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  screen_gram_kernel<<<ngs_blocks(n * 32, 256), 256, 0, (cudaStream_t)s>>>(
+      rows, phi, n, w, reinterpret_cast<const uint4*>(masks), rowptr, scale, vals);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+__global__ void screen_rhs_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi, int64_t n,
+                                  const float* __restrict__ w, const float* __restrict__ field, double scale,
+                                  double* __restrict__ rhs) {
+  const int64_t total = n * 27;
+  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
+    const int32_t r = rows[t];
+    if (r < 0) continue;
+    const int64_t p = t / 27;
+    double v = scale * (double)phi[t];
+    if (w) v *= (double)w[p];
+    if (field) v *= (double)field[p];
+    atomicAdd(rhs + r, v);
+  }
+}
+
+extern "C" int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, const float* w, double scale,
+                              double* rhs, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !phi || !rhs))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  screen_rhs_kernel<<<ngs_blocks(n * 27, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, w, nullptr, scale, rhs);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_correction_screen(const int32_t* rows, const float* phi, int64_t n, const float* w,
+                                     const float* field, double scale, double* rhs, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !phi || !field || !rhs))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  screen_rhs_kernel<<<ngs_blocks(n * 27, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, w, field, -scale, rhs);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- RHS from normals
+// target stride >= data stride: scatter from every data voxel to the 27 target voxels around the
+// target cell that holds the data voxel's centre (get_coords_neighbours, _hash_backend.py:194-228).
+__global__ void rhs_scatter_kernel(const int32_t* __restrict__ dc, int64_t nd, int sd, const float* __restrict__ nrm,
+                                   ngs_grid tg, const double* __restrict__ tc, const double* __restrict__ tgv,
+                                   int tab_len, double* __restrict__ rhs) {
+  const int st = tg.stride, M = st / sd;
+  for (int64_t i = ngs_gtid(); i < nd; i += ngs_gstride()) {
+    int q[3], c[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      c[a] = dc[i * 3 + a];
+      q[a] = (int)floorf(((float)c[a] + 0.5f * (float)sd) / (float)st) * st;
+    }
+    const double n0 = nrm[i * 3], n1 = nrm[i * 3 + 1], n2 = nrm[i * 3 + 2];
+    for (int kx = -1; kx <= 1; kx++)
+      for (int ky = -1; ky <= 1; ky++)
+        for (int kz = -1; kz <= 1; kz++) {
+          const int64_t t = grid_row(tg, q[0] + kx * st, q[1] + ky * st, q[2] + kz * st);
+          if (t < 0) continue;
+          const int k[3] = {kx, ky, kz};
+          double cv[3], gv[3];
+          bool ok = true;
+#pragma unroll
+          for (int a = 0; a < 3; a++) {
+            // rel = k*M + (q - c)/sd + (M-1)/2 ; idx = rel + (3M-1)/2  (integer)
+            const int idx = k[a] * M + (q[a] - c[a]) / sd + 2 * M - 1;
+            ok &= (idx >= 0 && idx < tab_len);
+            cv[a] = ok ? tc[idx] : 0.0;
+            gv[a] = ok ? tgv[idx] : 0.0;
+          }
+          if (!ok) continue;
+          const double v = n0 * gv[0] * cv[1] * cv[2] + n1 * cv[0] * gv[1] * cv[2] + n2 * cv[0] * cv[1] * gv[2];
+          atomicAdd(rhs + t, -v);
+        }
+  }
+}
+
+// target stride < data stride (coarse data, fine target): gather per target voxel over the coarse
+// data voxels whose centre lies within 1.5 fine voxels (the inverted map, _hash_backend.py:254-262).
+__global__ void rhs_gather_kernel(ngs_grid dg, const float* __restrict__ nrm, const int32_t* __restrict__ tcoords,
+                                  int64_t nt, int st, const double* __restrict__ tc, const double* __restrict__ tgv,
+                                  int tab_len, double* __restrict__ rhs) {
+  const int sd = dg.stride, M = sd / st;
+  for (int64_t i = ngs_gtid(); i < nt; i += ngs_gstride()) {
+    int q[3], c[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      c[a] = tcoords[i * 3 + a];
+      q[a] = (int)floorf(((float)c[a] + 0.5f * (float)st) / (float)sd) * sd;
+    }
+    double acc = 0.0;
+    for (int kx = -1; kx <= 1; kx++)
+      for (int ky = -1; ky <= 1; ky++)
+        for (int kz = -1; kz <= 1; kz++) {
+          const int k[3] = {kx, ky, kz};
+          double cv[3], gv[3];
+          bool ok = true;
+#pragma unroll
+          for (int a = 0; a < 3; a++) {
+            // nt = k*M + (q - c)/st + (M-1)/2 (fine units), keep |nt| < 1.5;
+            // rel = -nt * st / sd ; idx = rel * M + M/2 + 0.5 = -nt + M/2 + 0.5 (integer)
+            const int two_nt = 2 * (k[a] * M + (q[a] - c[a]) / st) + (M - 1);
+            ok &= (two_nt > -3 - 1 && two_nt < 3 + 1) && (abs(two_nt) <= 3);
+            const int idx = (-two_nt + M + 1) / 2;
+            ok &= (idx >= 0 && idx < tab_len);
+            cv[a] = ok ? tc[idx] : 0.0;
+            gv[a] = ok ? tgv[idx] : 0.0;
+          }
+          if (!ok) continue;
+          const int64_t d = grid_row(dg, q[0] + kx * sd, q[1] + ky * sd, q[2] + kz * sd);
+          if (d < 0) continue;
+          const double n0 = nrm[d * 3], n1 = nrm[d * 3 + 1], n2 = nrm[d * 3 + 2];
+          acc += n0 * gv[0] * cv[1] * cv[2] + n1 * cv[0] * gv[1] * cv[2] + n2 * cv[0] * cv[1] * gv[2];
+        }
+    rhs[i] -= acc;
+  }
+}
+
+extern "C" int ngs_rhs_normals(ngs_grid data_grid, const int32_t* data_coords, int64_t n_data, const float* normals,
+                               ngs_grid tgt_grid, const int32_t* tgt_coords, int64_t n_tgt, const double* tab_c,
+                               const double* tab_g, int tab_len, double* rhs, ngs_stream s) {
+  if (!normals || !tab_c || !tab_g || !rhs || tab_len <= 0) return NGS_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  if (tgt_grid.stride >= data_grid.stride) {
+    if (n_data <= 0) return NGS_OK;
+    if (!data_coords || !tgt_grid.words) return NGS_ERR_INVALID_ARG;
+    rhs_scatter_kernel<<<ngs_blocks(n_data, 128), 128, 0, st>>>(data_coords, n_data, data_grid.stride, normals,
+                                                               tgt_grid, tab_c, tab_g, tab_len, rhs);
+  } else {
+    if (n_tgt <= 0) return NGS_OK;
+    if (!tgt_coords || !data_grid.words) return NGS_ERR_INVALID_ARG;
+    rhs_gather_kernel<<<ngs_blocks(n_tgt, 128), 128, 0, st>>>(data_grid, normals, tgt_coords, n_tgt, tgt_grid.stride,
+                                                              tab_c, tab_g, tab_len, rhs);
+  }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- cross-level correction
+// rhs_fine[i] -= sum over the 125 coarse neighbours j of K(i, j) * x_coarse[j]
+// (reconstructor.py:153-168, stiffness part; computed matrix-free).
+__global__ void correction_kernel(const int32_t* __restrict__ fc, int64_t nf, int sf, ngs_grid cg,
+                                  const float* __restrict__ x, const double* __restrict__ tc,
+                                  const double* __restrict__ tg, int tab_len, double* __restrict__ rhs) {
+  extern __shared__ double tabs[];
+  for (int t = threadIdx.x; t < tab_len; t += blockDim.x) {
+    tabs[t] = tc[t];
+    tabs[tab_len + t] = tg[t];
+  }
+  __syncthreads();
+  const int sc = cg.stride, M = sc / sf;
+  for (int64_t i = ngs_gtid(); i < nf; i += ngs_gstride()) {
+    int q[3], base[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int c = fc[i * 3 + a];
+      q[a] = (int)floorf(((float)c + 0.5f * (float)sf) / (float)sc) * sc;
+      // idx = rel + 1.5M + 0.5 with rel = k*M + (q - c)/sf + (M-1)/2  ->  k*M + (q - c)/sf + 2M
+      base[a] = (q[a] - c) / sf + 2 * M;
+    }
+    double acc = 0.0;
+    for (int kx = -2; kx <= 2; kx++) {
+      const int ix = kx * M + base[0];
+      if (ix < 0 || ix >= tab_len) continue;
+      for (int ky = -2; ky <= 2; ky++) {
+        const int iy = ky * M + base[1];
+        if (iy < 0 || iy >= tab_len) continue;
+        for (int kz = -2; kz <= 2; kz++) {
+          const int iz = kz * M + base[2];
+          if (iz < 0 || iz >= tab_len) continue;
+          const int64_t j = grid_row(cg, q[0] + kx * sc, q[1] + ky * sc, q[2] + kz * sc);
+          if (j < 0) continue;
+          const double v = tabs[tab_len + ix] * tabs[iy] * tabs[iz] + tabs[ix] * tabs[tab_len + iy] * tabs[iz] +
+                           tabs[ix] * tabs[iy] * tabs[tab_len + iz];
+          acc += v * (double)x[j];
+        }
+      }
+    }
+    rhs[i] -= acc;
+  }
+}
+
+extern "C" int ngs_correction_stiffness(const int32_t* fine_coords, int64_t n_fine, int fine_stride, ngs_grid cg,
+                                        const float* x_coarse, const double* tab_c, const double* tab_g, int tab_len,
+                                        double* rhs, ngs_stream s) {
+  if (n_fine < 0 || fine_stride <= 0 || cg.stride <= fine_stride || tab_len <= 0 || tab_len > 4096) return NGS_ERR_INVALID_ARG;
+  if (n_fine == 0) return NGS_OK;
+  if (!fine_coords || !cg.words || !x_coarse || !tab_c || !tab_g || !rhs) return NGS_ERR_INVALID_ARG;
+  correction_kernel<<<ngs_blocks(n_fine, 128), 128, 2 * tab_len * sizeof(double), (cudaStream_t)s>>>(
+      fine_coords, n_fine, fine_stride, cg, x_coarse, tab_c, tab_g, tab_len, rhs);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- finish
+__global__ void finish_kernel(const double* __restrict__ v64, int64_t nnz, const int64_t* __restrict__ diag_slot,
+                              int64_t V, float* __restrict__ v32, float* __restrict__ inv_diag) {
+  for (int64_t i = ngs_gtid(); i < nnz; i += ngs_gstride()) v32[i] = (float)v64[i];
+  for (int64_t i = ngs_gtid(); i < V; i += ngs_gstride()) inv_diag[i] = (float)(1.0 / v64[diag_slot[i]]);
+}
+
+extern "C" int ngs_finish_system(const double* vals64, int64_t nnz, const int64_t* diag_slot, int64_t V, float* vals32,
+                                 float* inv_diag, ngs_stream s) {
+  if (nnz < 0 || V < 0 || (nnz > 0 && (!vals64 || !vals32)) || (V > 0 && (!diag_slot || !inv_diag)))
+    return NGS_ERR_INVALID_ARG;
+  if (nnz == 0 && V == 0) return NGS_OK;
+  finish_kernel<<<ngs_blocks(nnz > V ? nnz : V, 256), 256, 0, (cudaStream_t)s>>>(vals64, nnz, diag_slot, V, vals32,
+                                                                                inv_diag);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}

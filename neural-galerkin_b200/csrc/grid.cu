@@ -1,0 +1,372 @@
+// Rank-bitmap voxel index, density estimation, splatting and basis evaluation at points.
+#include "ngs_common.cuh"
+#include "scan.cuh"
+
+// ----------------------------------------------------------------------------- index build
+NGS_DEV void grid_set(const ngs_grid& g, int x, int y, int z) {
+  int bit;
+  const int64_t w = grid_word_index(g, x, y, z, &bit);
+  if (w < 0) return;
+  unsigned long long* bits = reinterpret_cast<unsigned long long*>(static_cast<char*>(g.words) + w * 16 + 8);
+  const unsigned long long m = 1ull << bit;
+  if (!(*reinterpret_cast<volatile unsigned long long*>(bits) & m)) atomicOr(bits, m);
+}
+
+// 8 trilinear corners of each point at the grid's stride (_hash_backend.py:469-510).
+__global__ void mark_points_kernel(ngs_grid g, const float* __restrict__ xyz, int64_t n, float inv_vs,
+                                   const int32_t* __restrict__ levels, int max_level) {
+  const float inv_s = 1.0f / (float)g.stride;
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    if (levels && levels[p] > max_level) continue;
+    int d[3], sg[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) tri_axis(q32(xyz[p * 3 + a], inv_vs), g.stride, inv_s, &d[a], &sg[a]);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int nx = (c >> 2) & 1, ny = (c >> 1) & 1, nz = c & 1;
+      grid_set(g, d[0] + nx * sg[0] * g.stride, d[1] + ny * sg[1] * g.stride, d[2] + nz * sg[2] * g.stride);
+    }
+  }
+}
+
+__global__ void mark_coords_kernel(ngs_grid g, const int32_t* __restrict__ c, int64_t n,
+                                   const int32_t* __restrict__ off, int n_off, int scale) {
+  const int64_t total = n * n_off;
+  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
+    const int64_t i = t / n_off;
+    const int o = (int)(t - i * n_off);
+    int ox = 0, oy = 0, oz = 0;
+    if (off) {
+      ox = off[o * 3] * scale;
+      oy = off[o * 3 + 1] * scale;
+      oz = off[o * 3 + 2] * scale;
+    }
+    grid_set(g, c[i * 3] + ox, c[i * 3 + 1] + oy, c[i * 3 + 2] + oz);
+  }
+}
+
+struct WordPopc {
+  const GridWord* w;
+  NGS_DEV int64_t operator()(int64_t i) const { return __popcll(w[i].bits); }
+};
+struct WordRank {
+  GridWord* w;
+  NGS_DEV void operator()(int64_t i, int64_t v) const { w[i].rank = (uint32_t)v; }
+};
+
+__global__ void emit_coords_kernel(ngs_grid g, int32_t* __restrict__ out) {
+  const GridWord* words = static_cast<const GridWord*>(g.words);
+  const int64_t per_x = (int64_t)g.dims[1] * g.zwords;
+  for (int64_t w = ngs_gtid(); w < g.nwords; w += ngs_gstride()) {
+    unsigned long long bits = words[w].bits;
+    if (!bits) continue;
+    int64_t r = words[w].rank;
+    const int i = (int)(w / per_x);
+    const int64_t rem = w - (int64_t)i * per_x;
+    const int j = (int)(rem / g.zwords);
+    const int kw = (int)(rem - (int64_t)j * g.zwords);
+    while (bits) {
+      const int b = __ffsll((long long)bits) - 1;
+      bits &= bits - 1;
+      const int k = kw * 64 + b;
+      out[r * 3] = g.origin[0] + i * g.stride;
+      out[r * 3 + 1] = g.origin[1] + j * g.stride;
+      out[r * 3 + 2] = g.origin[2] + k * g.stride;
+      r++;
+    }
+  }
+}
+
+__global__ void lookup_kernel(ngs_grid g, const int32_t* __restrict__ c, int64_t n, int64_t* __restrict__ rows) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) rows[i] = grid_row(g, c[i * 3], c[i * 3 + 1], c[i * 3 + 2]);
+}
+
+static bool grid_ok(const ngs_grid& g) {
+  return g.words && g.stride > 0 && (1 << g.log2_stride) == g.stride && g.dims[0] > 0 && g.dims[1] > 0 &&
+         g.dims[2] > 0 && g.zwords == (g.dims[2] + 63) / 64 &&
+         g.nwords == (int64_t)g.dims[0] * g.dims[1] * g.zwords &&
+         (reinterpret_cast<uintptr_t>(g.words) & 15u) == 0;
+}
+
+extern "C" int ngs_grid_mark_points(ngs_grid g, const float* xyz, int64_t n, float inv_vs, const int32_t* levels,
+                                    int max_level, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || (n > 0 && !xyz)) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  mark_points_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, levels, max_level);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_grid_mark_coords(ngs_grid g, const int32_t* coords, int64_t n, const int32_t* offsets, int n_off,
+                                    int offset_scale, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || (n > 0 && !coords)) return NGS_ERR_INVALID_ARG;
+  if (!offsets) n_off = 1;
+  if (n == 0 || n_off <= 0) return NGS_OK;
+  mark_coords_kernel<<<ngs_blocks(n * n_off, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, offsets, n_off,
+                                                                             offset_scale);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" size_t ngs_grid_workspace_bytes(const ngs_grid* g) { return g ? ngs_scan_ws_bytes(g->nwords) : 0; }
+
+extern "C" int ngs_grid_finalize(ngs_grid g, void* ws, size_t ws_bytes, int64_t* count_dev, ngs_stream s) {
+  if (!grid_ok(g)) return NGS_ERR_INVALID_ARG;
+  GridWord* w = static_cast<GridWord*>(g.words);
+  return ngs_scan(WordPopc{w}, WordRank{w}, g.nwords, count_dev, ws, ws_bytes, (cudaStream_t)s);
+}
+
+extern "C" int ngs_grid_emit_coords(ngs_grid g, int32_t* coords, ngs_stream s) {
+  if (!grid_ok(g) || !coords) return NGS_ERR_INVALID_ARG;
+  emit_coords_kernel<<<ngs_blocks(g.nwords, 256), 256, 0, (cudaStream_t)s>>>(g, coords);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_grid_lookup(ngs_grid g, const int32_t* coords, int64_t n, int64_t* rows, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || (n > 0 && (!coords || !rows))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  lookup_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, rows);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- trilinear splat
+// Corner cells from the fp32 quantisation; weights from the FP64 fractional position.
+struct Trilinear {
+  int d[3], sg[3];
+  float loc[3];
+};
+
+NGS_DEV Trilinear trilinear(const float* p, float inv_vs, double vs, int stride) {
+  Trilinear t;
+  const float inv_s = 1.0f / (float)stride;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    tri_axis(q32(p[a], inv_vs), stride, inv_s, &t.d[a], &t.sg[a]);
+    const double rel = (double)p[a] / vs - (double)t.d[a] - 0.5 * stride;
+    t.loc[a] = (float)(fabs(rel) / stride);
+  }
+  return t;
+}
+
+NGS_DEV float tri_weight(const Trilinear& t, int c) {
+  const int nx = (c >> 2) & 1, ny = (c >> 1) & 1, nz = c & 1;
+  return (nx ? t.loc[0] : 1.f - t.loc[0]) * (ny ? t.loc[1] : 1.f - t.loc[1]) * (nz ? t.loc[2] : 1.f - t.loc[2]);
+}
+
+__global__ void splat_kernel(ngs_grid g, const float* __restrict__ xyz, int64_t n, float inv_vs, double vs,
+                             const float* __restrict__ data, int dim, const float* __restrict__ pscale,
+                             const int32_t* __restrict__ levels, int level, float scale, float* __restrict__ out) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    if (levels && levels[p] != level) continue;
+    const Trilinear t = trilinear(xyz + p * 3, inv_vs, vs, g.stride);
+    const float ps = (pscale ? pscale[p] : 1.f) * scale;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int nx = (c >> 2) & 1, ny = (c >> 1) & 1, nz = c & 1;
+      const int64_t r = grid_row(g, t.d[0] + nx * t.sg[0] * g.stride, t.d[1] + ny * t.sg[1] * g.stride,
+                                 t.d[2] + nz * t.sg[2] * g.stride);
+      if (r < 0) continue;
+      const float w = tri_weight(t, c) * ps;
+      if (!data) {
+        atomicAdd(out + r, w);
+      } else {
+        for (int k = 0; k < dim; k++) atomicAdd(out + r * dim + k, w * data[p * dim + k]);
+      }
+    }
+  }
+}
+
+extern "C" int ngs_splat_weights(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, float* wd,
+                                 ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || (n > 0 && (!xyz || !wd))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  splat_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, nullptr, 1, nullptr,
+                                                                 nullptr, 0, 1.f, wd);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_splat_data(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, const float* data,
+                              int dim, const float* point_scale, const int32_t* levels, int level, float scale,
+                              float* out, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || dim < 1 || (n > 0 && (!xyz || !out))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  splat_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, data, dim, point_scale,
+                                                                 levels, level, scale, out);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- basis at points
+// Neighbourhood of a point at stride s (hashtree.py:168-181): quantised cell q and, per axis,
+// the position relative to the centre of cell q + k*s, in units of s, for k = -1, 0, 1.
+struct PointNbr {
+  int q[3];
+  float rel[3][3];
+};
+
+NGS_DEV PointNbr point_nbr(const float* p, float inv_vs, double vs, int stride) {
+  PointNbr r;
+  const float inv_s = 1.0f / (float)stride;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    r.q[a] = point_quant(q32(p[a], inv_vs), stride, inv_s);
+    const double pos = (double)p[a] / vs - 0.5;
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      r.rel[a][k] = (float)((pos - (double)r.q[a] - (double)((k - 1) * stride) - 0.5 * (stride - 1)) / stride);
+  }
+  return r;
+}
+
+__global__ void density_kernel(ngs_grid g, const float* __restrict__ xyz, int64_t n, float inv_vs, double vs,
+                               const float* __restrict__ wd, float inv_min_density, float inv_ln4, int depth,
+                               float* __restrict__ density, int32_t* __restrict__ levels, float* __restrict__ weight) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    const PointNbr nb = point_nbr(xyz + p * 3, inv_vs, vs, 1);
+    float bx[3], by[3], bz[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      bx[k] = bspline(nb.rel[0][k]);
+      by[k] = bspline(nb.rel[1][k]);
+      bz[k] = bspline(nb.rel[2][k]);
+    }
+    float acc = 0.f;
+    for (int kx = 0; kx < 3; kx++)
+      for (int ky = 0; ky < 3; ky++)
+        for (int kz = 0; kz < 3; kz++) {
+          const int64_t r = grid_row(g, nb.q[0] + kx - 1, nb.q[1] + ky - 1, nb.q[2] + kz - 1);
+          if (r >= 0) acc += bx[kx] * by[ky] * bz[kz] * wd[r];
+        }
+    const float rho = __fmul_rn(acc, 0.0625f);
+    if (density) density[p] = rho;
+    if (weight) weight[p] = __fdiv_rn(1.0f, rho);
+    if (levels) {
+      // -floor(log(rho / min_density) / ln 4), clamped (_hash_backend.py:428-429);
+      // both divisions by scalars run as products with fp32 reciprocals, as torch does on CUDA.
+      const float t = floorf(__fmul_rn(logf(__fmul_rn(rho, inv_min_density)), inv_ln4));
+      int lv = -(int)fminf(t, 0.f);
+      levels[p] = min(lv, depth - 1);
+    }
+  }
+}
+
+extern "C" int ngs_density_eval(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, const float* wd,
+                                float min_density, int depth, float* density, int32_t* levels, float* weight,
+                                ngs_stream s) {
+  if (!grid_ok(g) || g.stride != 1 || n < 0 || (n > 0 && (!xyz || !wd)) || min_density <= 0.f || depth < 1)
+    return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  const float inv_md = 1.0f / min_density;
+  const float inv_ln4 = 1.0f / (float)1.3862943611198906;
+  density_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, wd, inv_md, inv_ln4, depth,
+                                                                   density, levels, weight);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+__global__ void point_basis_kernel(ngs_grid g, const float* __restrict__ xyz, int64_t n, float inv_vs, double vs,
+                                   int32_t* __restrict__ rows, float* __restrict__ phi) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    const PointNbr nb = point_nbr(xyz + p * 3, inv_vs, vs, g.stride);
+    float bx[3], by[3], bz[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      bx[k] = bspline(nb.rel[0][k]);
+      by[k] = bspline(nb.rel[1][k]);
+      bz[k] = bspline(nb.rel[2][k]);
+    }
+    for (int kx = 0; kx < 3; kx++)
+      for (int ky = 0; ky < 3; ky++)
+        for (int kz = 0; kz < 3; kz++) {
+          const int o = kx * 9 + ky * 3 + kz;
+          const int64_t r = grid_row(g, nb.q[0] + (kx - 1) * g.stride, nb.q[1] + (ky - 1) * g.stride,
+                                     nb.q[2] + (kz - 1) * g.stride);
+          rows[p * 27 + o] = (int32_t)r;
+          phi[p * 27 + o] = r >= 0 ? bx[kx] * by[ky] * bz[kz] : 0.f;
+        }
+  }
+}
+
+extern "C" int ngs_point_basis(ngs_grid g, const float* xyz, int64_t n, float inv_vs, double vs, int32_t* rows,
+                               float* phi, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || (n > 0 && (!xyz || !rows || !phi))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  point_basis_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, rows, phi);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+__global__ void point_field_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi, int64_t n,
+                                   const float* __restrict__ x, float* __restrict__ out, int accumulate) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    float acc = 0.f;
+#pragma unroll 9
+    for (int k = 0; k < 27; k++) {
+      const int32_t r = rows[p * 27 + k];
+      if (r >= 0) acc += phi[p * 27 + k] * x[r];
+    }
+    out[p] = accumulate ? out[p] + acc : acc;
+  }
+}
+
+extern "C" int ngs_point_field(const int32_t* rows, const float* phi, int64_t n, const float* x, float* out,
+                               int accumulate, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !phi || !x || !out))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  point_field_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, x, out, accumulate);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// Field value / gradient at arbitrary positions, accumulated into out
+// (hashtree.py:157-192, bezier_tensor.py:56-73: the gradient is per finest-voxel unit / stride).
+__global__ void eval_field_kernel(ngs_grid g, const float* __restrict__ pos, int64_t n, float inv_vs, double vs,
+                                  const float* __restrict__ x, int grad, float* __restrict__ out) {
+  const float inv_s = 1.0f / (float)g.stride;
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    const PointNbr nb = point_nbr(pos + p * 3, inv_vs, vs, g.stride);
+    float b[3][3], db[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        b[a][k] = bspline(nb.rel[a][k]);
+        db[a][k] = bspline_d(nb.rel[a][k]) * inv_s;
+      }
+    float v = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    for (int kx = 0; kx < 3; kx++)
+      for (int ky = 0; ky < 3; ky++)
+        for (int kz = 0; kz < 3; kz++) {
+          const int64_t r = grid_row(g, nb.q[0] + (kx - 1) * g.stride, nb.q[1] + (ky - 1) * g.stride,
+                                     nb.q[2] + (kz - 1) * g.stride);
+          if (r < 0) continue;
+          const float xr = x[r];
+          if (!grad) {
+            v += b[0][kx] * b[1][ky] * b[2][kz] * xr;
+          } else {
+            gx += db[0][kx] * b[1][ky] * b[2][kz] * xr;
+            gy += b[0][kx] * db[1][ky] * b[2][kz] * xr;
+            gz += b[0][kx] * b[1][ky] * db[2][kz] * xr;
+          }
+        }
+    if (!grad) {
+      out[p] += v;
+    } else {
+      out[p * 3] += gx;
+      out[p * 3 + 1] += gy;
+      out[p * 3 + 2] += gz;
+    }
+  }
+}
+
+extern "C" int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv_vs, double vs, const float* x,
+                              int grad, float* out, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || (n > 0 && (!pos || !x || !out))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  eval_field_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(g, pos, n, inv_vs, vs, x, grad, out);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}

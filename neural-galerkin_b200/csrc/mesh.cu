@@ -1,0 +1,418 @@
+// Multi-level dual marching cubes (jspsr/core/reconstructor.py:296-397,
+// csrc/marching_cubes/dual_mc_inds.cu:45-182, dual_mc.cu:20-189).
+#include "ngs_common.cuh"
+#include "hash_table.cuh"
+
+// Triangle table (Lorensen / Bourke, data file) -- 256 cases x 16 edges, -1 terminated.
+__constant__ signed char c_tri[256][16] = {
+#include "mc_tables.inc"
+};
+// Edge endpoints in interpolation order (p1, p2); corner i of the MC cube sits at
+// (0,0,0),(1,0,0),(1,1,0),(0,1,0),(0,0,1),(1,0,1),(1,1,1),(0,1,1).
+__constant__ int c_edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+__constant__ int c_corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+// MC corner holding the octant (ox, oy, oz), indexed by ox + 2 oy + 4 oz.
+__constant__ int c_octant_slot[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+
+NGS_DEV int num_verts(int t) {
+  int n = 0;
+  while (n < 16 && c_tri[t][n] >= 0) n++;
+  return n;
+}
+
+NGS_DEV int cube_type(const float* v) {
+  int t = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) t |= (v[i] < 0.f ? 1 : 0) << i;
+  return t;
+}
+
+// Edge vertex with the reference's 1e-5 snapping rules; returns the weight of p1.
+NGS_DEV float sdf_interp(const float* p1, const float* p2, float v1, float v2, float* out) {
+  if (fabsf(v1) < 1.0e-5f) { out[0] = p1[0]; out[1] = p1[1]; out[2] = p1[2]; return 1.f; }
+  if (fabsf(v2) < 1.0e-5f) { out[0] = p2[0]; out[1] = p2[1]; out[2] = p2[2]; return 0.f; }
+  if (fabsf(v1 - v2) < 1.0e-5f) { out[0] = p1[0]; out[1] = p1[1]; out[2] = p1[2]; return 1.f; }
+  const float w2 = (0.0f - v1) / (v2 - v1);
+  const float w1 = 1.f - w2;
+#pragma unroll
+  for (int a = 0; a < 3; a++) out[a] = p1[a] * w1 + p2[a] * w2;
+  return w1;
+}
+
+// ----------------------------------------------------------------------------- dual corner accumulation
+template <typename Lookup>
+__global__ void dual_inds_kernel(Lookup lk, const int32_t* __restrict__ pb, int64_t n_primal, int stride, int depth,
+                                 int64_t idx_base, int32_t* __restrict__ acc, int32_t* __restrict__ cnt) {
+  const int sm1 = stride - 1;
+  const int64_t per = 8 + 12 * (int64_t)sm1 + 6 * (int64_t)sm1 * sm1;
+  const int64_t total = n_primal * per;
+  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
+    const int64_t pid = t / per;
+    int64_t q = t - pid * per;
+    int off[3];
+    int slots[4], ns;
+    if (q < 8) {
+      // corner (cx, cy, cz) = bits of q (x most significant): primal in the opposite octant
+      const int c[3] = {(int)(q >> 2) & 1, (int)(q >> 1) & 1, (int)q & 1};
+      for (int a = 0; a < 3; a++) off[a] = c[a] * stride;
+      slots[0] = c_octant_slot[(1 - c[0]) + 2 * (1 - c[1]) + 4 * (1 - c[2])];
+      ns = 1;
+    } else if (q < 8 + 12 * (int64_t)sm1) {
+      q -= 8;
+      const int e = (int)(q / sm1), tt = (int)(q % sm1) + 1;
+      const int ax = e >> 2, v0 = (e >> 1) & 1, v1 = e & 1;
+      const int b0 = ax == 0 ? 1 : 0, b1 = ax == 2 ? 1 : 2;
+      off[ax] = tt;
+      off[b0] = v0 * stride;
+      off[b1] = v1 * stride;
+      for (int o = 0; o < 2; o++) {
+        int oc[3];
+        oc[ax] = o;
+        oc[b0] = 1 - v0;
+        oc[b1] = 1 - v1;
+        slots[o] = c_octant_slot[oc[0] + 2 * oc[1] + 4 * oc[2]];
+      }
+      ns = 2;
+    } else {
+      q -= 8 + 12 * (int64_t)sm1;
+      const int64_t fc = (int64_t)sm1 * sm1;
+      const int f = (int)(q / fc);
+      const int64_t in = q % fc;
+      const int ax = f >> 1, side = f & 1;
+      const int b0 = ax == 0 ? 1 : 0, b1 = ax == 2 ? 1 : 2;
+      off[ax] = side * stride;
+      off[b0] = (int)(in % sm1) + 1;
+      off[b1] = (int)(in / sm1) + 1;
+      for (int o = 0; o < 4; o++) {
+        int oc[3];
+        oc[ax] = 1 - side;
+        oc[b0] = o & 1;
+        oc[b1] = o >> 1;
+        slots[o] = c_octant_slot[oc[0] + 2 * oc[1] + 4 * oc[2]];
+      }
+      ns = 4;
+    }
+    const int64_t row = lk(pb[pid * 3] + off[0], pb[pid * 3 + 1] + off[1], pb[pid * 3 + 2] + off[2]);
+    if (row < 0) continue;
+    // More than 8 slot writes into one dual cube is the reference's "Topology Error"
+    // (dual_mc_inds.cu:86,115,135): the writes are skipped and the count ends above 8,
+    // which the caller can detect from cnt.
+    const int before = atomicAdd(cnt + row, ns);
+    if (before >= 8) continue;
+    for (int i = 0; i < ns; i++) {
+      acc[(row * 8 + slots[i]) * 2] = (int32_t)(pid + idx_base);
+      acc[(row * 8 + slots[i]) * 2 + 1] = depth;
+    }
+  }
+}
+
+struct GridLookup {
+  ngs_grid g;
+  NGS_DEV int64_t operator()(int x, int y, int z) const { return grid_row(g, x, y, z); }
+};
+struct KeyLookup {
+  const Slot* slots;
+  int64_t mask;
+  NGS_DEV int64_t operator()(int x, int y, int z) const {
+    unsigned long long h = NGS_FNV_BASIS;
+    h = fnv_step(h, (unsigned)x);
+    h = fnv_step(h, (unsigned)y);
+    h = fnv_step(h, (unsigned)z);
+    return table_find_single(slots, mask, fnv_fold(h));
+  }
+};
+
+extern "C" int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_base, int64_t n_primal, int stride,
+                                        int depth, int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s) {
+  if (!dual.words || stride < 1 || n_primal < 0 || (n_primal > 0 && (!primal_base || !acc || !cnt)))
+    return NGS_ERR_INVALID_ARG;
+  if (n_primal == 0) return NGS_OK;
+  const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
+  dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
+      GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, cnt);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_t* primal_base, int64_t n_primal,
+                                        int stride, int depth, int64_t idx_base, int32_t* acc, int32_t* cnt,
+                                        ngs_stream s) {
+  if (!dual || !dual->slots || stride < 1 || n_primal < 0 || (n_primal > 0 && (!primal_base || !acc || !cnt)))
+    return NGS_ERR_INVALID_ARG;
+  if (n_primal == 0) return NGS_OK;
+  const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
+  dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
+      KeyLookup{static_cast<const Slot*>(dual->slots), dual->nslots - 1}, primal_base, n_primal, stride, depth,
+      idx_base, acc, cnt);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+__global__ void select_kernel(const int32_t* __restrict__ cnt, int64_t n, int32_t* __restrict__ keep) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) keep[i] = cnt[i] == 8 ? 1 : 0;
+}
+
+__global__ void compact_acc_kernel(const int32_t* __restrict__ acc, const int32_t* __restrict__ keep,
+                                   const int64_t* __restrict__ off, int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
+    if (!keep[i]) continue;
+    const int4* src = reinterpret_cast<const int4*>(acc + i * 16);
+    int4* dst = reinterpret_cast<int4*>(out + off[i] * 16);
+#pragma unroll
+    for (int k = 0; k < 4; k++) dst[k] = src[k];
+  }
+}
+
+extern "C" int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!cnt || !keep))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  select_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(cnt, n, keep);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, const int64_t* keep_offset, int64_t n,
+                                   int32_t* acc_out, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!acc || !keep || !keep_offset || !acc_out))) return NGS_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(acc_out)) & 15u) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  compact_acc_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(acc, keep, keep_offset, n, acc_out);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- dual MC
+__global__ void dual_count_kernel(const int32_t* __restrict__ acc, int64_t m, const float* __restrict__ values,
+                                  int32_t* __restrict__ vcount) {
+  for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = values[acc[(c * 8 + i) * 2]];
+    vcount[c] = num_verts(cube_type(v));
+  }
+}
+
+__global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int64_t m, const float* __restrict__ pos,
+                                 const float* __restrict__ values, const int64_t* __restrict__ voff,
+                                 float* __restrict__ tris, int32_t* __restrict__ vids) {
+  for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
+    int id[8];
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      id[i] = acc[(c * 8 + i) * 2];
+      v[i] = values[id[i]];
+    }
+    const int t = cube_type(v);
+    const int64_t base = voff[c];
+    for (int k = 0; k < 16 && c_tri[t][k] >= 0; k++) {
+      const int e = c_tri[t][k];
+      const int a = c_edge[e][0], b = c_edge[e][1];
+      const float p1[3] = {pos[id[a] * 3], pos[id[a] * 3 + 1], pos[id[a] * 3 + 2]};
+      const float p2[3] = {pos[id[b] * 3], pos[id[b] * 3 + 1], pos[id[b] * 3 + 2]};
+      float out[3];
+      sdf_interp(p1, p2, v[a], v[b], out);
+      const int64_t o = base + k;
+      tris[o * 3] = out[0];
+      tris[o * 3 + 1] = out[1];
+      tris[o * 3 + 2] = out[2];
+      vids[o * 2] = max(id[a], id[b]);
+      vids[o * 2 + 1] = min(id[a], id[b]);
+    }
+  }
+}
+
+extern "C" int ngs_dual_mc_count(const int32_t* acc, int64_t n_cubes, const float* values, int32_t* vcount,
+                                 ngs_stream s) {
+  if (n_cubes < 0 || (n_cubes > 0 && (!acc || !values || !vcount))) return NGS_ERR_INVALID_ARG;
+  if (n_cubes == 0) return NGS_OK;
+  dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, n_cubes, values, vcount);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_dual_mc_emit(const int32_t* acc, int64_t n_cubes, const float* pos, const float* values,
+                                const int64_t* voffset, float* tris, int32_t* vert_ids, ngs_stream s) {
+  if (n_cubes < 0 || (n_cubes > 0 && (!acc || !pos || !values || !voffset || !tris || !vert_ids)))
+    return NGS_ERR_INVALID_ARG;
+  if (n_cubes == 0) return NGS_OK;
+  dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, n_cubes, pos, values, voffset, tris,
+                                                                        vert_ids);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- vertex de-duplication
+__global__ void vd_count_kernel(const int32_t* __restrict__ vids, int64_t n, int32_t* __restrict__ cnt) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) atomicAdd(cnt + vids[i * 2], 1);
+}
+
+__global__ void vd_scatter_kernel(const int32_t* __restrict__ vids, int64_t n, const int64_t* __restrict__ start,
+                                  int32_t* __restrict__ fill, int64_t* __restrict__ sorted) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
+    const int32_t b = vids[i * 2];
+    const int32_t pos = atomicAdd(fill + b, 1);
+    sorted[start[b] + pos] = ((int64_t)vids[i * 2 + 1] << 32) | (int64_t)i;
+  }
+}
+
+// Sort each bucket by (vid1, key index) and flag the first key of every distinct vid1.
+__global__ void vd_sort_kernel(const int64_t* __restrict__ start, const int32_t* __restrict__ count, int64_t nb,
+                               int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
+  for (int64_t b = ngs_gtid(); b < nb; b += ngs_gstride()) {
+    const int64_t s0 = start[b];
+    const int c = count[b];
+    for (int i = 1; i < c; i++) {
+      const int64_t key = sorted[s0 + i];
+      int j = i - 1;
+      while (j >= 0 && sorted[s0 + j] > key) {
+        sorted[s0 + j + 1] = sorted[s0 + j];
+        j--;
+      }
+      sorted[s0 + j + 1] = key;
+    }
+    for (int i = 0; i < c; i++)
+      first[s0 + i] = (i == 0 || (sorted[s0 + i] >> 32) != (sorted[s0 + i - 1] >> 32)) ? 1 : 0;
+  }
+}
+
+__global__ void vd_emit_kernel(const int32_t* __restrict__ vids, const float* __restrict__ tris, int64_t n,
+                               const int64_t* __restrict__ start, const int32_t* __restrict__ count,
+                               const int64_t* __restrict__ sorted, const int64_t* __restrict__ vertex_id,
+                               int64_t* __restrict__ faces, float* __restrict__ verts) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
+    const int32_t b = vids[i * 2];
+    const int64_t v1 = vids[i * 2 + 1];
+    int64_t lo = start[b], hi = start[b] + count[b] - 1;
+    // first position whose vid1 >= v1
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if ((sorted[mid] >> 32) < v1) lo = mid + 1; else hi = mid;
+    }
+    const int64_t vid = vertex_id[lo];
+    faces[i] = vid;
+    if ((sorted[lo] & 0xffffffffll) == i) {
+      verts[vid * 3] = tris[i * 3];
+      verts[vid * 3 + 1] = tris[i * 3 + 1];
+      verts[vid * 3 + 2] = tris[i * 3 + 2];
+    }
+  }
+}
+
+extern "C" int ngs_vdedup_count(const int32_t* vert_ids, int64_t n_keys, int32_t* bucket_count, ngs_stream s) {
+  if (n_keys < 0 || (n_keys > 0 && (!vert_ids || !bucket_count))) return NGS_ERR_INVALID_ARG;
+  if (n_keys == 0) return NGS_OK;
+  if (n_keys > 0x7fffffffLL) return NGS_ERR_INVALID_ARG;
+  vd_count_kernel<<<ngs_blocks(n_keys, 256), 256, 0, (cudaStream_t)s>>>(vert_ids, n_keys, bucket_count);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_vdedup_sort(const int32_t* vert_ids, int64_t n_keys, const int64_t* bucket_start, int64_t n_buckets,
+                               int32_t* bucket_fill, int64_t* sorted_keys, int32_t* first, ngs_stream s) {
+  if (n_keys < 0 || n_buckets < 0 || (n_keys > 0 && (!vert_ids || !bucket_start || !bucket_fill || !sorted_keys || !first)))
+    return NGS_ERR_INVALID_ARG;
+  if (n_keys == 0) return NGS_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  vd_scatter_kernel<<<ngs_blocks(n_keys, 256), 256, 0, st>>>(vert_ids, n_keys, bucket_start, bucket_fill, sorted_keys);
+  vd_sort_kernel<<<ngs_blocks(n_buckets, 128), 128, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_vdedup_emit(const int32_t* vert_ids, const float* tris, int64_t n_keys, const int64_t* bucket_start,
+                               const int32_t* bucket_count, const int64_t* sorted_keys, const int64_t* vertex_id,
+                               int64_t* faces, float* vertices, ngs_stream s) {
+  if (n_keys < 0 || (n_keys > 0 && (!vert_ids || !tris || !bucket_start || !bucket_count || !sorted_keys ||
+                                    !vertex_id || !faces || !vertices)))
+    return NGS_ERR_INVALID_ARG;
+  if (n_keys == 0) return NGS_OK;
+  vd_emit_kernel<<<ngs_blocks(n_keys, 256), 256, 0, (cudaStream_t)s>>>(vert_ids, tris, n_keys, bucket_start,
+                                                                     bucket_count, sorted_keys, vertex_id, faces,
+                                                                     vertices);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- conformal tree helpers
+__global__ void children_kernel(const int32_t* __restrict__ par, int64_t n, int stride, int32_t* __restrict__ out) {
+  const int64_t total = n * 8;
+  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
+    const int64_t p = t >> 3;
+    const int c = (int)(t & 7);
+    out[t * 3] = par[p * 3] + ((c >> 2) & 1) * stride;
+    out[t * 3 + 1] = par[p * 3 + 1] + ((c >> 1) & 1) * stride;
+    out[t * 3 + 2] = par[p * 3 + 2] + (c & 1) * stride;
+  }
+}
+
+__global__ void leaf_kernel(const int32_t* __restrict__ cells, int64_t n, ngs_grid g, int32_t* __restrict__ leaf) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride())
+    leaf[i] = g.words ? (grid_row(g, cells[i * 3], cells[i * 3 + 1], cells[i * 3 + 2]) < 0 ? 1 : 0) : 1;
+}
+
+__global__ void compact_coords_kernel(const int32_t* __restrict__ c, const int32_t* __restrict__ keep,
+                                      const int64_t* __restrict__ off, int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
+    if (!keep[i]) continue;
+    const int64_t o = off[i];
+    out[o * 3] = c[i * 3];
+    out[o * 3 + 1] = c[i * 3 + 1];
+    out[o * 3 + 2] = c[i * 3 + 2];
+  }
+}
+
+__global__ void expand_kernel(const int32_t* __restrict__ c, int64_t n, int n_up, int stride, float evs,
+                              int32_t* __restrict__ out, float* __restrict__ pos) {
+  const int e3 = n_up * n_up * n_up;
+  const int64_t total = n * e3;
+  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
+    const int64_t i = t / e3;
+    const int e = (int)(t - i * e3);
+    const int ex = e / (n_up * n_up), ey = (e / n_up) % n_up, ez = e % n_up;
+    const int v[3] = {c[i * 3] * n_up + ex * stride, c[i * 3 + 1] * n_up + ey * stride, c[i * 3 + 2] * n_up + ez * stride};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      out[t * 3 + a] = v[a];
+      if (pos) pos[t * 3 + a] = __fmul_rn((float)(v[a] + stride), evs);
+    }
+  }
+}
+
+extern "C" int ngs_conformal_children(const int32_t* parents, int64_t n_parents, int stride, int32_t* children,
+                                      ngs_stream s) {
+  if (n_parents < 0 || (n_parents > 0 && (!parents || !children))) return NGS_ERR_INVALID_ARG;
+  if (n_parents == 0) return NGS_OK;
+  children_kernel<<<ngs_blocks(n_parents * 8, 256), 256, 0, (cudaStream_t)s>>>(parents, n_parents, stride, children);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_leaf_flags(const int32_t* cells, int64_t n, ngs_grid finer_parents, int32_t* leaf, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!cells || !leaf))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  leaf_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(cells, n, finer_parents, leaf);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_compact_coords(const int32_t* coords, const int32_t* keep, const int64_t* keep_offset, int64_t n,
+                                  int32_t* out, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!coords || !keep || !keep_offset || !out))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  compact_coords_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(coords, keep, keep_offset, n, out);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_expand_cells(const int32_t* cells, int64_t n, int n_up, int stride, float evs, int32_t* out,
+                                float* pos, ngs_stream s) {
+  if (n < 0 || n_up < 1 || (n > 0 && (!cells || !out))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  expand_kernel<<<ngs_blocks(n * n_up * n_up * n_up, 256), 256, 0, (cudaStream_t)s>>>(cells, n, n_up, stride, evs, out,
+                                                                                     pos);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}

@@ -1,0 +1,210 @@
+"""ctypes binding of libngs.so (the C ABI declared in include/ngs.h).
+
+The library is built in-tree by ``neural-galerkin_b200/build.py``.  There is no
+CPU fallback: every op raises if the library is missing or if a CUDA call
+fails, with the library's status message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "libngs.so"
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "buffer or workspace too small", 3: "hash insert failed",
+          4: "not converged", 5: "topology error", 6: "CUDA error", 7: "device-side wait timed out"}
+NGS_OK, NGS_ERR_NOT_CONVERGED, NGS_ERR_TIMEOUT = 0, 4, 7
+PCG_REFERENCE, PCG_MIXED, PCG_FP64 = 0, 1, 2
+
+vp, i32, i64, f32, f64, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_double, C.c_size_t
+
+
+class Grid(C.Structure):
+    _fields_ = [("origin", C.c_int32 * 3), ("dims", C.c_int32 * 3), ("stride", C.c_int32),
+                ("log2_stride", C.c_int32), ("zwords", C.c_int32), ("pad_", C.c_int32),
+                ("nwords", C.c_int64), ("words", C.c_void_p)]
+
+
+class HashTable(C.Structure):
+    _fields_ = [("slots", C.c_void_p), ("nslots", C.c_int64), ("inserted", C.c_int64)]
+
+
+class PcgSystem(C.Structure):
+    _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("rowptr", vp), ("cols", vp), ("vals32", vp),
+                ("vals64", vp), ("b32", vp), ("b64", vp), ("inv_diag", vp), ("x32", vp), ("x64", vp)]
+
+
+class PcgConfig(C.Structure):
+    _fields_ = [("mode", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double), ("res_fix", C.c_int),
+                ("replace_every", C.c_int), ("blocks", C.c_int), ("timeout_s", C.c_double)]
+
+
+G, H = Grid, C.POINTER(HashTable)
+_SIGS = {
+    "ngs_status_string": ([C.c_int], C.c_char_p),
+    "ngs_last_cuda_error": ([], C.c_char_p),
+    "ngs_version": ([], C.c_int),
+    "ngs_hash_coords": ([vp, C.c_int, i64, C.c_int, vp, vp], C.c_int),
+    "ngs_kernel_hash": ([vp, C.c_int, i64, C.c_int, vp, i64, vp, vp], C.c_int),
+    "ngs_hash_table_slots": ([i64, C.c_int], i64),
+    "ngs_hash_table_build": ([H, vp, vp, i64, vp, vp], C.c_int),
+    "ngs_hash_table_query": ([H, vp, i64, vp, vp], C.c_int),
+    "ngs_hash_table_query_coords": ([H, vp, i64, vp, vp], C.c_int),
+    "ngs_scan_workspace_bytes": ([i64], sz),
+    "ngs_exclusive_scan_i64": ([vp, i64, vp, vp, vp, sz, vp], C.c_int),
+    "ngs_exclusive_scan_i32": ([vp, i64, vp, vp, vp, sz, vp], C.c_int),
+    "ngs_points_bbox": ([vp, i64, vp, vp], C.c_int),
+    "ngs_grid_mark_points": ([G, vp, i64, f32, vp, C.c_int, vp], C.c_int),
+    "ngs_grid_mark_coords": ([G, vp, i64, vp, C.c_int, C.c_int, vp], C.c_int),
+    "ngs_grid_workspace_bytes": ([C.POINTER(Grid)], sz),
+    "ngs_grid_finalize": ([G, vp, sz, vp, vp], C.c_int),
+    "ngs_grid_emit_coords": ([G, vp, vp], C.c_int),
+    "ngs_grid_lookup": ([G, vp, i64, vp, vp], C.c_int),
+    "ngs_splat_weights": ([G, vp, i64, f32, f64, vp, vp], C.c_int),
+    "ngs_density_eval": ([G, vp, i64, f32, f64, vp, f32, C.c_int, vp, vp, vp, vp], C.c_int),
+    "ngs_splat_data": ([G, vp, i64, f32, f64, vp, C.c_int, vp, vp, C.c_int, f32, vp, vp], C.c_int),
+    "ngs_point_basis": ([G, vp, i64, f32, f64, vp, vp, vp], C.c_int),
+    "ngs_point_field": ([vp, vp, i64, vp, vp, C.c_int, vp], C.c_int),
+    "ngs_eval_field": ([G, vp, i64, f32, f64, vp, C.c_int, vp, vp], C.c_int),
+    "ngs_weighted_sum": ([vp, vp, i64, vp, vp], C.c_int),
+    "ngs_stencil_count": ([G, vp, i64, vp, vp, vp], C.c_int),
+    "ngs_stencil_fill": ([G, vp, i64, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_screen_gram": ([vp, vp, i64, vp, vp, vp, f64, vp, vp], C.c_int),
+    "ngs_screen_rhs": ([vp, vp, i64, vp, f64, vp, vp], C.c_int),
+    "ngs_rhs_normals": ([G, vp, i64, vp, G, vp, i64, vp, vp, C.c_int, vp, vp], C.c_int),
+    "ngs_correction_stiffness": ([vp, i64, C.c_int, G, vp, vp, vp, C.c_int, vp, vp], C.c_int),
+    "ngs_correction_screen": ([vp, vp, i64, vp, vp, f64, vp, vp], C.c_int),
+    "ngs_finish_system": ([vp, i64, vp, i64, vp, vp, vp], C.c_int),
+    "ngs_pcg_workspace_bytes": ([i64, C.c_int], sz),
+    "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
+    "ngs_spmv64": ([i64, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_dot64": ([vp, vp, i64, vp, vp], C.c_int),
+    "ngs_axpby64": ([i64, f64, vp, f64, vp, vp], C.c_int),
+    "ngs_mul64": ([i64, vp, vp, vp, vp], C.c_int),
+    "ngs_sparse_meshgrid": ([vp, vp, vp, vp, vp, i64, vp, vp, vp], C.c_int),
+    "ngs_screened_multiplication": ([H, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, i64, vp, vp], C.c_int),
+    "ngs_screened_multiplication_backward": ([H, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, i64, vp, vp, vp,
+                                              vp, vp], C.c_int),
+    "ngs_ddi_forward": ([vp, vp, vp, vp, vp, i64, C.c_int, C.c_int, vp, vp, vp], C.c_int),
+    "ngs_ddi_backward": ([vp, vp, vp, vp, vp, vp, vp, i64, C.c_int, C.c_int, vp, vp, vp], C.c_int),
+    "ngs_primal_mc_count": ([vp, i64, C.c_int, vp, vp], C.c_int),
+    "ngs_primal_mc_emit": ([vp, vp, i64, C.c_int, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_indices_grid": ([G, vp, i64, C.c_int, C.c_int, i64, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_indices_hash": ([H, vp, i64, C.c_int, C.c_int, i64, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_select": ([vp, i64, vp, vp], C.c_int),
+    "ngs_dual_mc_compact": ([vp, vp, vp, i64, vp, vp], C.c_int),
+    "ngs_dual_mc_count": ([vp, i64, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_emit": ([vp, i64, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_vdedup_count": ([vp, i64, vp, vp], C.c_int),
+    "ngs_vdedup_sort": ([vp, i64, vp, i64, vp, vp, vp, vp], C.c_int),
+    "ngs_vdedup_emit": ([vp, vp, i64, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_conformal_children": ([vp, i64, C.c_int, vp, vp], C.c_int),
+    "ngs_leaf_flags": ([vp, i64, G, vp, vp], C.c_int),
+    "ngs_compact_coords": ([vp, vp, vp, i64, vp, vp], C.c_int),
+    "ngs_expand_cells": ([vp, i64, C.c_int, C.c_int, f32, vp, vp, vp], C.c_int),
+}
+
+_lib = None
+
+
+def load():
+    """Load libngs.so and attach prototypes (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"libngs.so not found at {LIB_PATH}; build it with neural-galerkin_b200/build.py")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (args, ret) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.argtypes, fn.restype = args, ret
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+class NgsError(RuntimeError):
+    def __init__(self, status, where):
+        lib = load()
+        msg = lib.ngs_status_string(status).decode()
+        if status == 6:
+            msg += ": " + lib.ngs_last_cuda_error().decode()
+        super().__init__(f"{where}: {msg}")
+        self.status = status
+
+
+def call(name, *args):
+    """Call a libngs entry point; raise NgsError on a non-OK status."""
+    rc = getattr(load(), name)(*args)
+    if rc != NGS_OK:
+        raise NgsError(rc, name)
+    return rc
+
+
+def require_cuda(t: torch.Tensor, name="tensor"):
+    if not t.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor (libngs has no CPU path)")
+
+
+def ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+# ----------------------------------------------------------------------------- helpers
+def scan(values: torch.Tensor, out: torch.Tensor = None, total: torch.Tensor = None):
+    """Exclusive prefix sum (int32 or int64 values) -> int64; returns (out, total_dev)."""
+    n = values.numel()
+    out = torch.empty(n, dtype=torch.int64, device=values.device) if out is None else out
+    total = torch.empty(1, dtype=torch.int64, device=values.device) if total is None else total
+    ws_bytes = load().ngs_scan_workspace_bytes(n)
+    ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=values.device)
+    fn = "ngs_exclusive_scan_i64" if values.dtype == torch.int64 else "ngs_exclusive_scan_i32"
+    call(fn, ptr(values), n, ptr(out), ptr(total), ptr(ws), ws_bytes, stream())
+    return out, total
+
+
+def make_grid(origin, dims, stride, device) -> tuple[Grid, torch.Tensor]:
+    """A zeroed rank-bitmap over the box origin + [0, dims) * stride."""
+    stride = int(stride)
+    assert stride > 0 and stride & (stride - 1) == 0
+    dims = [max(int(d), 1) for d in dims]
+    zwords = (dims[2] + 63) // 64
+    nwords = dims[0] * dims[1] * zwords
+    if nwords > (1 << 33):
+        raise RuntimeError(f"voxel index box too large ({dims} cells at stride {stride})")
+    words = torch.zeros(nwords * 2, dtype=torch.int64, device=device)
+    g = Grid()
+    for a in range(3):
+        g.origin[a] = int(origin[a])
+        g.dims[a] = dims[a]
+    g.stride, g.log2_stride, g.zwords, g.nwords = stride, int(math.log2(stride)), zwords, nwords
+    g.words = words.data_ptr()
+    return g, words
+
+
+def grid_finalize(g: Grid, words: torch.Tensor, count: torch.Tensor):
+    ws_bytes = load().ngs_grid_workspace_bytes(C.byref(g))
+    ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=words.device)
+    call("ngs_grid_finalize", g, ptr(ws), ws_bytes, ptr(count), stream())
+    return ws
+
+
+def null_grid() -> Grid:
+    g = Grid()
+    g.stride, g.log2_stride, g.zwords, g.nwords, g.words = 1, 0, 1, 0, None
+    return g
+
+
+def f32_inv(vs: float) -> float:
+    """fp32(1 / fp32(vs)): the reciprocal torch multiplies by when dividing by a Python float on CUDA."""
+    return float(np.float32(1.0) / np.float32(vs))

@@ -1,0 +1,145 @@
+"""1-D integral tables of the quadratic B-spline basis, derived exactly.
+
+The reference ships these as ``jspsr/data/bezier_integrals.pkl``
+(``jspsr/bases/bezier_tensor.py:26-34``), a file that was never published.  The
+tables follow from the basis definition (``bezier_tensor.py:17-22``) and the
+index conventions of ``bezier_tensor.py:75-121``; every entry is the integral
+of a piecewise polynomial, evaluated here exactly (antiderivatives of the
+polynomial pieces between consecutive knots).  Level ratios beyond the
+reference's 16 (``n_multiples=5``) follow from the same formulas.
+
+Names and meaning (M = 2**m is the stride ratio of the two levels):
+
+* ``ssi[m][i] = int B(y + dx) B(y / M) dy``,             ``dx = -1.5M - 0.5 + i``
+* ``sdi[m][i] = int B'(y + dx) B'(y / M) dy``            (no chain factor; the caller divides by the coarse stride)
+* ``dpi[m][i] = int_{ra}^{ra+1} B(x / M) dx``,           ``ra = 1.5M - 1 - i``
+* ``pi[m][i]  = int_{ra}^{ra+1} B'(x / M) dx``           (no chain factor)
+* ``idpi[m-1][i] = int_{max(ra,-1.5)}^{min(ra+M,1.5)} B(x) dx``,  ``ra = 0.5 - i``
+* ``ipi[m-1][i]  = int ... B'(x) dx``
+"""
+from __future__ import annotations
+
+from functools import lru_cache
+
+import numpy as np
+from numpy.polynomial import polynomial as P
+
+# B-spline pieces on [-1.5,-0.5), [-0.5,0.5), [0.5,1.5): coefficients in ascending powers.
+_KNOTS = (-1.5, -0.5, 0.5, 1.5)
+_PIECES = (np.array([2.25, 3.0, 1.0]), np.array([1.5, 0.0, -2.0]), np.array([2.25, -3.0, 1.0]))
+
+
+def _piece(x_lo, x_hi, scale=1.0, shift=0.0, deriv=False):
+    """Pieces of B(scale * y + shift) (or d/du B(u) at u = scale*y + shift) as polynomials in y."""
+    out = []
+    for (a, b), c in zip(zip(_KNOTS[:-1], _KNOTS[1:]), _PIECES):
+        poly = P.polyder(c) if deriv else c
+        # u = scale * y + shift  ->  y in [(a - shift) / scale, (b - shift) / scale]
+        lo, hi = (a - shift) / scale, (b - shift) / scale
+        comp = np.zeros(1)
+        for k, ck in enumerate(poly):
+            comp = P.polyadd(comp, ck * P.polypow([shift, scale], k))
+        out.append((lo, hi, comp))
+    return out
+
+
+def _integrate_product(f_pieces, g_pieces=None, lo=-np.inf, hi=np.inf):
+    total = 0.0
+    if g_pieces is None:
+        g_pieces = [(-np.inf, np.inf, np.array([1.0]))]
+    for fl, fh, fp in f_pieces:
+        for gl, gh, gp in g_pieces:
+            a, b = max(fl, gl, lo), min(fh, gh, hi)
+            if b <= a:
+                continue
+            anti = P.polyint(P.polymul(fp, gp))
+            total += P.polyval(b, anti) - P.polyval(a, anti)
+    return total
+
+
+@lru_cache(maxsize=None)
+def shifted(m: int):
+    """(ssi[m], sdi[m]) as float64 arrays of length 3M + 2."""
+    M = 2 ** m
+    ssi, sdi = [], []
+    for i in range(3 * M + 2):
+        dx = -1.5 * M - 0.5 + i
+        ssi.append(_integrate_product(_piece(0, 0, 1.0, dx), _piece(0, 0, 1.0 / M, 0.0)))
+        sdi.append(_integrate_product(_piece(0, 0, 1.0, dx, True), _piece(0, 0, 1.0 / M, 0.0, True)))
+    return np.array(ssi), np.array(sdi)
+
+
+@lru_cache(maxsize=None)
+def partial(m: int):
+    """(dpi[m], pi[m]) as float64 arrays of length 3M."""
+    M = 2 ** m
+    dpi, pi = [], []
+    for i in range(3 * M):
+        ra = 1.5 * M - 1 - i
+        dpi.append(_integrate_product(_piece(0, 0, 1.0 / M, 0.0), None, ra, ra + 1))
+        pi.append(_integrate_product(_piece(0, 0, 1.0 / M, 0.0, True), None, ra, ra + 1))
+    return np.array(dpi), np.array(pi)
+
+
+@lru_cache(maxsize=None)
+def inverse_partial(m: int):
+    """(idpi[m-1], ipi[m-1]) for m >= 1 as float64 arrays of length M + 2."""
+    assert m >= 1
+    M = 2 ** m
+    f, df = [], []
+    for i in range(M + 2):
+        ra = 0.5 - i
+        lb, ub = max(ra, -1.5), min(ra + M, 1.5)
+        f.append(_integrate_product(_piece(0, 0), None, lb, ub) if ub > lb else 0.0)
+        df.append(_integrate_product(_piece(0, 0, deriv=True), None, lb, ub) if ub > lb else 0.0)
+    return np.array(f), np.array(df)
+
+
+def ratio_log2(m_ratio: int) -> int:
+    m = int(m_ratio).bit_length() - 1
+    assert 2 ** m == m_ratio, m_ratio
+    return m
+
+
+# ----------------------------------------------------------------------------- kernel-ready tables
+def stencil125(stride: int) -> np.ndarray:
+    """Same-level stiffness of the 125 lexicographic offsets (dx, dy, dz) in [-2, 2]^3."""
+    ssi, sdi = shifted(0)
+    c = ssi * stride
+    g = sdi / stride
+    out = np.zeros(125)
+    o = 0
+    for dx in range(-2, 3):
+        for dy in range(-2, 3):
+            for dz in range(-2, 3):
+                ix, iy, iz = dx + 2, dy + 2, dz + 2
+                out[o] = g[ix] * c[iy] * c[iz] + c[ix] * g[iy] * c[iz] + c[ix] * c[iy] * g[iz]
+                o += 1
+    return out
+
+
+def correction_tables(fine_stride: int, coarse_stride: int):
+    """(tc, tg) for K(fine, coarse): tc = ssi * s_fine, tg = sdi / s_coarse (length 3M + 2)."""
+    ssi, sdi = shifted(ratio_log2(coarse_stride // fine_stride))
+    return ssi * fine_stride, sdi / coarse_stride
+
+
+def rhs_tables(data_stride: int, target_stride: int):
+    """(tc, tg) for the divergence RHS of a data level onto a target level."""
+    if target_stride >= data_stride:
+        M = target_stride // data_stride
+        dpi, pi = partial(ratio_log2(M))
+        return dpi * data_stride, pi * (data_stride / target_stride)
+    M = data_stride // target_stride
+    idpi, ipi = inverse_partial(ratio_log2(M))
+    return idpi * target_stride, ipi
+
+
+def reference_pickle_tables(n_mult: int = 5):
+    """The eight tables in the order of the reference's pickle (bezier_tensor.py:31-34)."""
+    sh = [shifted(m) for m in range(n_mult)]
+    pa = [partial(m) for m in range(n_mult)]
+    inv = [inverse_partial(m) for m in range(1, n_mult)]
+    return ([p[1] for p in pa], [p[0] for p in pa], [p[1] for p in inv], [p[0] for p in inv],
+            [s[0] for s in sh], [s[1] for s in sh], [np.zeros_like(s[0]) for s in sh],
+            [np.zeros_like(p[0]) for p in inv])

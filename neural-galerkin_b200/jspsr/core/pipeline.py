@@ -1,0 +1,513 @@
+"""Device-resident screened-Poisson reconstruction on libngs kernels.
+
+This is the B200 path behind ``jspsr.reconstruct`` (``jspsr/__init__.py:8-61`` of
+the reference).  It keeps the reference's formulation step for step --
+density-adaptive octree (``_hash_backend.py:414-444``), splatted normals
+(``__init__.py:40-48``), coarse-to-fine Galerkin solve with cross-level
+correction and screening (``reconstructor.py:79-195``), mean-chi level set and
+multi-level dual marching cubes (``reconstructor.py:296-397``) -- but the data
+structures are new:
+
+* each level is a rank bitmap (``ngs_grid``): voxel rows are lexicographic ranks,
+  so sorted coordinates, inverse maps and neighbour lookups need no sort and no hash;
+* the level matrix is a CSR over the 5x5x5 stencil with a per-row offset mask; the
+  screening Gram is added in place from the points (no pair hash table);
+* the cross-level correction is matrix-free (stiffness by stencil lookups,
+  screening through the coarse field at the points);
+* each level is solved by one persistent PCG kernel (FP32 SpMV, FP64 dots,
+  FP64 residual replacement / refinement).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .. import _lib as L
+from ..bases import tables as TB
+
+CONFORM_OFFSETS = torch.tensor([(0, 0, 0), (0, 0, 1), (0, 1, 0), (0, 1, 1),
+                                (1, 0, 0), (1, 0, 1), (1, 1, 0), (1, 1, 1)], dtype=torch.int32)
+
+
+# ----------------------------------------------------------------------------- solver spec
+@dataclass
+class SolverSpec:
+    """Parsed solver string, e.g. ``"pcg@tol=1e-7@maxiter=300"`` (grammar of ``solver.py:180-186``)."""
+    name: str = "pcg-mixed"
+    tol: float = 1.0e-7
+    maxiter: int = -1
+    res_fix: bool = False
+    replace: int = 50
+    timeout: float = 30.0
+
+    @property
+    def mode(self):
+        return {"pcg": L.PCG_REFERENCE, "pcg-mixed": L.PCG_MIXED, "pcg-fp64": L.PCG_FP64,
+                "plain-fp64": None}[self.name]
+
+
+def parse_solver(spec: str) -> SolverSpec:
+    """Parse ``name@key=value@...`` without ``eval``; ``cholmod`` / ``mixed`` map to an FP64 solve."""
+    parts = spec.split("@")
+    name = parts[0]
+    out = SolverSpec(name=name)
+    if name == "pcg":
+        out.tol, out.maxiter = 1.0e-5, -1          # solver.py:192-196 defaults
+    elif name in ("cholmod", "mixed"):
+        out.name, out.tol, out.maxiter = "pcg-fp64", 1.0e-12, -1
+    elif name not in ("pcg-mixed", "pcg-fp64", "plain-fp64"):
+        raise NotImplementedError(f"unknown solver {name!r}")
+    for kv in parts[1:]:
+        k, v = kv.split("=", 1)
+        k = k.strip()
+        if k == "tol":
+            out.tol = float(v)
+        elif k == "maxiter":
+            out.maxiter = int(float(v))
+        elif k == "res_fix":
+            out.res_fix = v.strip().lower() in ("1", "true", "yes")
+        elif k == "replace":
+            out.replace = int(v)
+        elif k == "timeout":
+            out.timeout = float(v)
+        elif k == "verbose":
+            pass
+        else:
+            raise ValueError(f"unknown solver option {k!r}")
+    return out
+
+
+# ----------------------------------------------------------------------------- levels
+@dataclass
+class Level:
+    stride: int
+    grid: L.Grid
+    words: torch.Tensor
+    coords: torch.Tensor = None
+    n: int = 0
+    # system
+    masks: torch.Tensor = None
+    rowptr: torch.Tensor = None
+    cols: torch.Tensor = None
+    vals64: torch.Tensor = None
+    vals32: torch.Tensor = None
+    diag_slot: torch.Tensor = None
+    inv_diag: torch.Tensor = None
+    nnz: int = 0
+    rows: torch.Tensor = None      # point basis [N, 27]
+    phi: torch.Tensor = None
+    normals: torch.Tensor = None   # splatted normal data (points with this exact level)
+    rhs: torch.Tensor = None
+    x64: torch.Tensor = None
+    x32: torch.Tensor = None
+    info: torch.Tensor = None
+    resid: torch.Tensor = None
+
+
+def _box(qmin, qmax, stride, pad=1):
+    """Cell box [lo, hi] (multiples of stride) covering the trilinear corners of points in [qmin, qmax]."""
+    s = np.float32(stride)
+    lo = (np.floor(qmin / s) * s).astype(np.int64) - pad * stride
+    hi = (np.floor(qmax / s) * s).astype(np.int64) + pad * stride
+    dims = (hi - lo) // stride + 1
+    return lo, dims
+
+
+@dataclass
+class Timings:
+    events: list = field(default_factory=list)
+
+    def mark(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.events.append((name, e))
+
+    def summary(self):
+        torch.cuda.synchronize()
+        out = {}
+        for (n0, e0), (n1, e1) in zip(self.events[:-1], self.events[1:]):
+            out[n1] = out.get(n1, 0.0) + e0.elapsed_time(e1)
+        return out
+
+
+class Reconstruction:
+    """One reconstruction, every buffer device-resident."""
+
+    def __init__(self, xyz: torch.Tensor, normal: torch.Tensor, voxel_size: float, depth: int = 4,
+                 min_density: float = 32.0, screen_alpha: float = 4.0, screen_delta: float = 0.1,
+                 solver: str = "pcg-mixed@tol=1e-7", timings: Timings | None = None):
+        L.require_cuda(xyz, "xyz")
+        L.require_cuda(normal, "normal")
+        self.xyz = xyz.contiguous().float()
+        self.nrm = normal.contiguous().float()
+        self.n = self.xyz.shape[0]
+        if self.n == 0:
+            raise ValueError("empty point cloud")
+        self.vs = float(voxel_size)
+        self.depth = int(depth)
+        self.min_density = float(min_density)
+        self.alpha = float(screen_alpha)
+        self.delta = float(screen_delta)
+        self.solver = parse_solver(solver)
+        self.dev = self.xyz.device
+        self.inv_vs = L.f32_inv(self.vs)
+        self.levels: list[Level] = []
+        self.t = timings
+        self.solve_stats = {}
+
+    def _mark(self, name):
+        if self.t is not None:
+            self.t.mark(name)
+
+    # ------------------------------------------------------------------ tree
+    def build_tree(self):
+        """Density, point levels and the per-level rank bitmaps (_hash_backend.py:13-28,414-444)."""
+        st = L.stream()
+        self._mark("start")
+        bbox = torch.empty(6, dtype=torch.float32, device=self.dev)
+        L.call("ngs_points_bbox", L.ptr(self.xyz), self.n, L.ptr(bbox), st)
+        b = bbox.cpu().numpy()
+        self.bbox = b
+        # density at voxel 4 * vs (hashtree.py:283-285): stride-1 grid of that voxel size
+        vsd = 4.0 * self.vs
+        inv_d = L.f32_inv(vsd)
+        qd = [np.float32(b[:3]) * np.float32(inv_d), np.float32(b[3:]) * np.float32(inv_d)]
+        lo, dims = _box(qd[0], qd[1], 1)
+        gd, wd_words = L.make_grid(lo, dims, 1, self.dev)
+        L.call("ngs_grid_mark_points", gd, L.ptr(self.xyz), self.n, np.float32(inv_d), None, 0, st)
+        cnt = torch.empty(1, dtype=torch.int64, device=self.dev)
+        L.grid_finalize(gd, wd_words, cnt)
+        wd = torch.zeros(8 * self.n, dtype=torch.float32, device=self.dev)
+        L.call("ngs_splat_weights", gd, L.ptr(self.xyz), self.n, np.float32(inv_d), vsd, L.ptr(wd), st)
+        self.density = torch.empty(self.n, dtype=torch.float32, device=self.dev)
+        self.point_level = torch.empty(self.n, dtype=torch.int32, device=self.dev)
+        self.weight = torch.empty(self.n, dtype=torch.float32, device=self.dev)
+        L.call("ngs_density_eval", gd, L.ptr(self.xyz), self.n, np.float32(inv_d), vsd, L.ptr(wd),
+               np.float32(self.min_density), self.depth, L.ptr(self.density), L.ptr(self.point_level),
+               L.ptr(self.weight), st)
+        self._mark("density")
+        # level grids
+        q = [np.float32(b[:3]) * np.float32(self.inv_vs), np.float32(b[3:]) * np.float32(self.inv_vs)]
+        counts = torch.empty(self.depth, dtype=torch.int64, device=self.dev)
+        self._ws = []
+        for d in range(self.depth):
+            s = 2 ** d
+            lo, dims = _box(q[0], q[1], s)
+            g, words = L.make_grid(lo, dims, s, self.dev)
+            L.call("ngs_grid_mark_points", g, L.ptr(self.xyz), self.n, np.float32(self.inv_vs),
+                   L.ptr(self.point_level), d, st)
+            self._ws.append(L.grid_finalize(g, words, counts[d:d + 1]))
+            self.levels.append(Level(stride=s, grid=g, words=words))
+        hist = torch.bincount(self.point_level.long(), minlength=self.depth)
+        host = torch.cat([counts, hist]).cpu().numpy()
+        self.level_hist = host[self.depth:]
+        for d, lv in enumerate(self.levels):
+            lv.n = int(host[d])
+            if lv.n == 0:
+                raise ValueError(f"level {d} of the hierarchy is empty; lower min_density")
+            lv.coords = torch.empty((lv.n, 3), dtype=torch.int32, device=self.dev)
+            L.call("ngs_grid_emit_coords", lv.grid, L.ptr(lv.coords), st)
+        self._mark("tree")
+        return self
+
+    # ------------------------------------------------------------------ assembly
+    def assemble(self):
+        """Splat normals, point basis, per-level CSR structure, stiffness and screening Gram."""
+        st = L.stream()
+        inv = np.float32(self.inv_vs)
+        for d, lv in enumerate(self.levels):
+            if self.level_hist[d] > 0:
+                lv.normals = torch.zeros((lv.n, 3), dtype=torch.float32, device=self.dev)
+                L.call("ngs_splat_data", lv.grid, L.ptr(self.xyz), self.n, inv, self.vs, L.ptr(self.nrm), 3,
+                       L.ptr(self.weight), L.ptr(self.point_level), d, np.float32(1.0 / lv.stride ** 3),
+                       L.ptr(lv.normals), st)
+            lv.rows = torch.empty((self.n, 27), dtype=torch.int32, device=self.dev)
+            lv.phi = torch.empty((self.n, 27), dtype=torch.float32, device=self.dev)
+            L.call("ngs_point_basis", lv.grid, L.ptr(self.xyz), self.n, inv, self.vs, L.ptr(lv.rows), L.ptr(lv.phi), st)
+            lv.masks = torch.empty((lv.n, 4), dtype=torch.int32, device=self.dev)
+            counts = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
+            L.call("ngs_stencil_count", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(counts), st)
+            lv.rowptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
+            L.scan(counts, out=lv.rowptr[:lv.n], total=lv.rowptr[lv.n:])
+        self._mark("structure")
+        nnz = torch.stack([lv.rowptr[lv.n] for lv in self.levels]).cpu().numpy()
+        for d, lv in enumerate(self.levels):
+            lv.nnz = int(nnz[d])
+            lv.cols = torch.empty(lv.nnz, dtype=torch.int32, device=self.dev)
+            lv.vals64 = torch.empty(lv.nnz, dtype=torch.float64, device=self.dev)
+            lv.diag_slot = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
+            st125 = torch.from_numpy(TB.stencil125(lv.stride)).to(self.dev)
+            L.call("ngs_stencil_fill", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(lv.rowptr),
+                   L.ptr(st125), L.ptr(lv.cols), L.ptr(lv.vals64), L.ptr(lv.diag_slot), st)
+            if self.alpha > 0:
+                sf = 0.25 ** d
+                L.call("ngs_screen_gram", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(lv.masks),
+                       L.ptr(lv.rowptr), sf * self.alpha, L.ptr(lv.vals64), st)
+            lv.vals32 = torch.empty(lv.nnz, dtype=torch.float32, device=self.dev)
+            lv.inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
+            L.call("ngs_finish_system", L.ptr(lv.vals64), lv.nnz, L.ptr(lv.diag_slot), lv.n, L.ptr(lv.vals32),
+                   L.ptr(lv.inv_diag), st)
+        self._mark("assembly")
+        return self
+
+    # ------------------------------------------------------------------ RHS + solve
+    def _rhs(self, d):
+        st = L.stream()
+        lv = self.levels[d]
+        rhs = torch.zeros(lv.n, dtype=torch.float64, device=self.dev)
+        for dd, ld in enumerate(self.levels):
+            if ld.normals is None:
+                continue
+            tc, tg = TB.rhs_tables(ld.stride, lv.stride)
+            tc = torch.from_numpy(tc).to(self.dev)
+            tg = torch.from_numpy(tg).to(self.dev)
+            L.call("ngs_rhs_normals", ld.grid, L.ptr(ld.coords), ld.n, L.ptr(ld.normals), lv.grid, L.ptr(lv.coords),
+                   lv.n, L.ptr(tc), L.ptr(tg), tc.numel(), L.ptr(rhs), st)
+        sf = 0.25 ** d
+        if self.alpha > 0:
+            L.call("ngs_screen_rhs", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, sf * self.alpha * self.delta,
+                   L.ptr(rhs), st)
+        coarser = list(range(self.depth - 1, d, -1))
+        if coarser:
+            if self.alpha > 0:
+                fieldp = torch.zeros(self.n, dtype=torch.float32, device=self.dev)
+                for dd in coarser:
+                    lc = self.levels[dd]
+                    L.call("ngs_point_field", L.ptr(lc.rows), L.ptr(lc.phi), self.n, L.ptr(lc.x32), L.ptr(fieldp), 1, st)
+                L.call("ngs_correction_screen", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(fieldp),
+                       sf * self.alpha, L.ptr(rhs), st)
+            for dd in coarser:
+                lc = self.levels[dd]
+                tc, tg = TB.correction_tables(lv.stride, lc.stride)
+                tc = torch.from_numpy(tc).to(self.dev)
+                tg = torch.from_numpy(tg).to(self.dev)
+                L.call("ngs_correction_stiffness", L.ptr(lv.coords), lv.n, lv.stride, lc.grid, L.ptr(lc.x32),
+                       L.ptr(tc), L.ptr(tg), tc.numel(), L.ptr(rhs), st)
+        lv.rhs = rhs
+        return rhs
+
+    def _solve_level(self, lv: Level):
+        spec = self.solver
+        lv.x32 = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
+        lv.x64 = torch.empty(lv.n, dtype=torch.float64, device=self.dev)
+        lv.info = torch.zeros(4, dtype=torch.int64, device=self.dev)
+        lv.resid = torch.zeros(2, dtype=torch.float64, device=self.dev)
+        if spec.mode is None:
+            return self._solve_plain_fp64(lv)
+        sysd = L.PcgSystem()
+        sysd.n, sysd.nnz = lv.n, lv.nnz
+        sysd.rowptr, sysd.cols, sysd.inv_diag = lv.rowptr.data_ptr(), lv.cols.data_ptr(), lv.inv_diag.data_ptr()
+        sysd.vals32, sysd.vals64 = lv.vals32.data_ptr(), lv.vals64.data_ptr()
+        b32 = lv.rhs.float()
+        sysd.b32, sysd.b64 = b32.data_ptr(), lv.rhs.data_ptr()
+        sysd.x32, sysd.x64 = lv.x32.data_ptr(), lv.x64.data_ptr()
+        cfg = L.PcgConfig()
+        cfg.mode, cfg.max_iter, cfg.tol = spec.mode, spec.maxiter, spec.tol
+        cfg.res_fix, cfg.replace_every, cfg.blocks, cfg.timeout_s = int(spec.res_fix), spec.replace, 0, spec.timeout
+        ws_bytes = L.load().ngs_pcg_workspace_bytes(lv.n, spec.mode)
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.dev)
+        L.call("ngs_pcg_solve", L.C.byref(sysd), L.C.byref(cfg), L.ptr(ws), ws_bytes, L.ptr(lv.info),
+               L.ptr(lv.resid), L.stream())
+        if spec.mode == L.PCG_REFERENCE:
+            lv.x64 = lv.x32.double()
+        lv._keep = (ws, b32)
+
+    def _solve_plain_fp64(self, lv: Level):
+        """Host-driven FP64 Jacobi-PCG, one launch per vector op and a host check per iteration --
+        the 'plain GPU' comparator following the reference loop (solve_pcg.cu:80-128)."""
+        spec, st, n = self.solver, L.stream(), lv.n
+        A = (lv.rowptr, lv.cols, lv.vals64)
+        dinv = (1.0 / lv.vals64[lv.diag_slot])
+        b = lv.rhs
+        x = torch.zeros(n, dtype=torch.float64, device=self.dev)
+        r = b.clone()
+        p = torch.zeros_like(x)
+        q = torch.empty_like(x)
+        z = torch.empty_like(x)
+        dot = torch.empty(1, dtype=torch.float64, device=self.dev)
+
+        def dotv(a, c):
+            L.call("ngs_dot64", L.ptr(a), L.ptr(c), n, L.ptr(dot), st)
+            return float(dot.item())
+        atol = spec.tol * math.sqrt(dotv(b, b))
+        rho, it = 0.0, 0
+        while spec.maxiter < 0 or it < spec.maxiter:
+            L.call("ngs_mul64", n, L.ptr(dinv), L.ptr(r), L.ptr(z), st)
+            rho1, rho = rho, dotv(r, z)
+            if it == 0:
+                p.copy_(z)
+            else:
+                L.call("ngs_axpby64", n, 1.0, L.ptr(z), rho / rho1, L.ptr(p), st)
+            L.call("ngs_spmv64", n, L.ptr(A[0]), L.ptr(A[1]), L.ptr(A[2]), L.ptr(p), L.ptr(q), st)
+            alpha = rho / dotv(p, q)
+            L.call("ngs_axpby64", n, alpha, L.ptr(p), 1.0, L.ptr(x), st)
+            L.call("ngs_axpby64", n, -alpha, L.ptr(q), 1.0, L.ptr(r), st)
+            it += 1
+            if math.sqrt(dotv(r, r)) <= atol:
+                break
+        lv.x64 = x
+        lv.x32.copy_(x)
+        lv.info[0] = it
+
+    def solve(self):
+        """Coarse-to-fine solve (reconstructor.py:122-189)."""
+        for d in range(self.depth - 1, -1, -1):
+            self._rhs(d)
+            self._solve_level(self.levels[d])
+        self._mark("solve")
+        return self
+
+    def check_solves(self):
+        """Read back iteration counts / status of every level (one sync)."""
+        info = torch.stack([lv.info for lv in self.levels]).cpu().numpy()
+        resid = torch.stack([lv.resid for lv in self.levels]).cpu().numpy()
+        self.solve_stats = {d: dict(iters=int(info[d, 0]), status=int(info[d, 1]), replacements=int(info[d, 2]),
+                                    resid=float(resid[d, 0]), bnorm=float(resid[d, 1])) for d in range(self.depth)}
+        for d, s in self.solve_stats.items():
+            if s["status"] not in (L.NGS_OK, L.NGS_ERR_NOT_CONVERGED):
+                raise L.NgsError(s["status"], f"PCG level {d}")
+        return self.solve_stats
+
+    # ------------------------------------------------------------------ field
+    def chi_raw(self, pos: torch.Tensor, grad: bool = False) -> torch.Tensor:
+        """Sum over levels of the interpolated field at positions (reconstructor.py:197-226)."""
+        pos = pos.contiguous().float()
+        out = torch.zeros((pos.shape[0], 3) if grad else pos.shape[0], dtype=torch.float32, device=self.dev)
+        for lv in self.levels:
+            L.call("ngs_eval_field", lv.grid, L.ptr(pos), pos.shape[0], np.float32(self.inv_vs), self.vs,
+                   L.ptr(lv.x32), int(grad), L.ptr(out), L.stream())
+        return out
+
+    def mean_chi(self) -> torch.Tensor:
+        """Density-weighted mean of chi at the input points (reconstructor.py:228-236), as a device scalar."""
+        chi = torch.zeros(self.n, dtype=torch.float32, device=self.dev)
+        for lv in self.levels:
+            L.call("ngs_point_field", L.ptr(lv.rows), L.ptr(lv.phi), self.n, L.ptr(lv.x32), L.ptr(chi), 1, L.stream())
+        sums = torch.empty(2, dtype=torch.float64, device=self.dev)
+        L.call("ngs_weighted_sum", L.ptr(chi), L.ptr(self.weight), self.n, L.ptr(sums), L.stream())
+        self.chi_points = chi
+        return (sums[0] / sums[1]).float()
+
+    # ------------------------------------------------------------------ mesh
+    def extract_mesh(self, n_upsample: int = 2):
+        """Multi-level dual marching cubes (reconstructor.py:296-397)."""
+        st = L.stream()
+        dev = self.dev
+        mean = self.mean_chi()
+        max_depth = self.depth
+        q = [np.float32(self.bbox[:3]) * np.float32(self.inv_vs), np.float32(self.bbox[3:]) * np.float32(self.inv_vs)]
+        base, leaf_flags, parent_grids = {}, {}, {}
+        for d in range(max_depth):
+            lv = self.levels[d]
+            s = lv.stride
+            if d < max_depth - 1:
+                # parents at 2s of the level's voxels, then all 8 children of each parent
+                lo, dims = _box(q[0], q[1], 2 * s, pad=2)
+                pg, pw = L.make_grid(lo, dims, 2 * s, dev)
+                L.call("ngs_grid_mark_coords", pg, L.ptr(lv.coords), lv.n, None, 1, 0, st)
+                pc = torch.empty(1, dtype=torch.int64, device=dev)
+                ws = L.grid_finalize(pg, pw, pc)
+                npar = int(pc.item())
+                parents = torch.empty((npar, 3), dtype=torch.int32, device=dev)
+                L.call("ngs_grid_emit_coords", pg, L.ptr(parents), st)
+                cells = torch.empty((npar * 8, 3), dtype=torch.int32, device=dev)
+                L.call("ngs_conformal_children", L.ptr(parents), npar, s, L.ptr(cells), st)
+                parent_grids[d] = (pg, pw, ws)
+            else:
+                cells = lv.coords
+            if d > 0:
+                leaf = torch.empty(cells.shape[0], dtype=torch.int32, device=dev)
+                pg = parent_grids[d - 1][0]
+                L.call("ngs_leaf_flags", L.ptr(cells), cells.shape[0], pg, L.ptr(leaf), st)
+                off, tot = L.scan(leaf)
+                nleaf = int(tot.item())
+                if nleaf == 0:
+                    max_depth = d
+                    break
+                leaf_flags[d] = (leaf, off, nleaf)
+            base[d] = cells
+        for d in range(1, max_depth):
+            leaf, off, nleaf = leaf_flags[d]
+            out = torch.empty((nleaf, 3), dtype=torch.int32, device=dev)
+            L.call("ngs_compact_coords", L.ptr(base[d]), L.ptr(leaf), L.ptr(off), base[d].shape[0], L.ptr(out), st)
+            base[d] = out
+        self._mark("leaves")
+        # expanded primal cells and their sample positions
+        evs = np.float32(self.vs / n_upsample)
+        e3 = n_upsample ** 3
+        counts = [base[d].shape[0] * e3 for d in range(max_depth)]
+        total = sum(counts)
+        epb = torch.empty((total, 3), dtype=torch.int32, device=dev)
+        pos = torch.empty((total, 3), dtype=torch.float32, device=dev)
+        starts = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        for d in range(max_depth):
+            L.call("ngs_expand_cells", L.ptr(base[d]), base[d].shape[0], n_upsample, self.levels[d].stride, evs,
+                   L.ptr(epb[starts[d]:]), L.ptr(pos[starts[d]:]), st)
+        # dual centres: unique corners of all expanded cells
+        lo = np.full(3, np.iinfo(np.int64).max)
+        hi = np.full(3, np.iinfo(np.int64).min)
+        for d in range(max_depth):
+            s = self.levels[d].stride
+            g = self.levels[d].grid
+            glo = np.array(g.origin[:], dtype=np.int64)
+            ghi = glo + (np.array(g.dims[:], dtype=np.int64) - 1) * s
+            lo = np.minimum(lo, n_upsample * (glo - 2 * s))
+            hi = np.maximum(hi, n_upsample * (ghi + 3 * s))
+        dg, dw = L.make_grid(lo, (hi - lo) + 1, 1, dev)
+        offs = CONFORM_OFFSETS.to(dev)
+        for d in range(max_depth):
+            L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
+                   self.levels[d].stride, st)
+        dcount = torch.empty(1, dtype=torch.int64, device=dev)
+        self._dual_ws = L.grid_finalize(dg, dw, dcount)
+        nd = int(dcount.item())
+        acc = torch.zeros((nd, 8, 2), dtype=torch.int32, device=dev)
+        cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
+        for d in range(max_depth):
+            L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride, d,
+                   int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
+        keep = torch.empty(nd, dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
+        koff, ktot = L.scan(keep)
+        m = int(ktot.item())
+        acc_c = torch.empty((m, 8, 2), dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_compact", L.ptr(acc), L.ptr(keep), L.ptr(koff), nd, L.ptr(acc_c), st)
+        self.topology_overflow = cnt  # counts above 8 mark the reference's "Topology Error"
+        self._mark("dual grid")
+        # field at the primal samples
+        vals = self.chi_raw(pos) - mean
+        self._mark("chi")
+        # marching cubes
+        vcount = torch.empty(m, dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_count", L.ptr(acc_c), m, L.ptr(vals), L.ptr(vcount), st)
+        voff, vtot = L.scan(vcount)
+        nv = int(vtot.item())
+        tris = torch.empty((nv, 3), dtype=torch.float32, device=dev)
+        vids = torch.empty((nv, 2), dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_emit", L.ptr(acc_c), m, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris), L.ptr(vids), st)
+        # vertex de-duplication by (vid0, vid1) (reconstructor.py:380-383)
+        bcount = torch.zeros(total, dtype=torch.int32, device=dev)
+        L.call("ngs_vdedup_count", L.ptr(vids), nv, L.ptr(bcount), st)
+        bstart, _ = L.scan(bcount)
+        fill = torch.zeros(total, dtype=torch.int32, device=dev)
+        sorted_keys = torch.empty(nv, dtype=torch.int64, device=dev)
+        first = torch.empty(nv, dtype=torch.int32, device=dev)
+        L.call("ngs_vdedup_sort", L.ptr(vids), nv, L.ptr(bstart), total, L.ptr(fill), L.ptr(sorted_keys),
+               L.ptr(first), st)
+        vid_of, nvert_t = L.scan(first)
+        nvert = int(nvert_t.item())
+        faces = torch.empty(nv, dtype=torch.int64, device=dev)
+        verts = torch.empty((nvert, 3), dtype=torch.float32, device=dev)
+        L.call("ngs_vdedup_emit", L.ptr(vids), L.ptr(tris), nv, L.ptr(bstart), L.ptr(fill), L.ptr(sorted_keys),
+               L.ptr(vid_of), L.ptr(faces), L.ptr(verts), st)
+        self._mark("mesh")
+        self.mesh_info = dict(n_primal=total, n_dual=nd, n_cubes=m, max_depth=max_depth, acc=acc_c, values=vals,
+                              positions=pos, counts=counts)
+        return verts, faces.view(-1, 3)
+
+    def run(self, n_upsample: int = 2):
+        self.build_tree().assemble().solve()
+        return self.extract_mesh(n_upsample)

@@ -411,7 +411,7 @@ def evaluate_chi_raw(sol: Solution, pos32: np.ndarray, pos64=None, grad=False):
         pts, vx, rel = point_neighbours(g, q32, q64, range_kernel(3))
         if grad:
             b = [bspline(rel[:, i]) for i in range(3)]
-            db = [bspline_d(rel[:, i]) / (g.stride * sol.vs) for i in range(3)]
+            db = [bspline_d(rel[:, i]) / g.stride for i in range(3)]   # bezier_tensor.py:70-72
             val = np.stack([db[0] * b[1] * b[2], b[0] * db[1] * b[2], b[0] * b[1] * db[2]], 1) * xd[vx, None]
             np.add.at(out, pts, val)
         else:

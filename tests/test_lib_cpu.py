@@ -1,0 +1,75 @@
+"""CPU-side checks of the native library: it loads and exports every symbol include/ngs.h declares."""
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def header_symbols():
+    text = (ROOT / "include" / "ngs.h").read_text()
+    return sorted(set(re.findall(r"\b(ngs_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_header_symbols():
+    from jspsr import _lib
+    lib = _lib.load()
+    missing = [s for s in header_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    from jspsr import _lib
+    assert set(header_symbols()) == set(_lib.exported_symbols())
+
+
+def test_status_strings():
+    from jspsr import _lib
+    lib = _lib.load()
+    assert lib.ngs_status_string(0) == b"ok"
+    assert b"tolerance" in lib.ngs_status_string(4)
+    assert lib.ngs_version() >= 10000
+
+
+def test_solver_spec_grammar():
+    from jspsr.core.pipeline import parse_solver
+    s = parse_solver("pcg@tol=1e-7@maxiter=300")
+    assert (s.name, s.tol, s.maxiter) == ("pcg", 1e-7, 300)
+    s = parse_solver("pcg")
+    assert (s.tol, s.maxiter) == (1e-5, -1)
+    s = parse_solver("pcg-mixed@tol=1e-9@replace=25")
+    assert (s.mode, s.tol, s.replace) == (1, 1e-9, 25)
+    with pytest.raises(ValueError):
+        parse_solver("pcg@tol=__import__('os')")
+    with pytest.raises(NotImplementedError):
+        parse_solver("cg-magic")
+
+
+def test_product_tables_match_oracle():
+    import numpy as np
+    from jspsr.bases import tables as P
+    from oracle import tables as T
+    t = T.bezier_tables(5)
+    for m in range(5):
+        M = 2 ** m
+        s, d = P.shifted(m)
+        np.testing.assert_allclose(s, t["SHIFTED_SELF_INTEGRAL"][m], rtol=1e-10, atol=1e-11)
+        np.testing.assert_allclose(d, t["SHIFTED_DERIVATIVE_INTEGRAL"][m], rtol=1e-10, atol=1e-11)
+        f, g = P.partial(m)
+        np.testing.assert_allclose(f, t["DERIVATIVE_PARTIAL_INTEGRAL"][m], atol=1e-11)
+        np.testing.assert_allclose(g, t["PARTIAL_INTEGRAL"][m], atol=1e-11)
+        if m:
+            f, g = P.inverse_partial(m)
+            np.testing.assert_allclose(f, t["INV_DERIVATIVE_PARTIAL_INTEGRAL"][m - 1], atol=1e-11)
+            np.testing.assert_allclose(g, t["INV_PARTIAL_INTEGRAL"][m - 1], atol=1e-11)
+
+
+def test_stencil_is_symmetric_and_annihilates_nothing():
+    import numpy as np
+    from jspsr.bases import tables as P
+    st = P.stencil125(1).reshape(5, 5, 5)
+    np.testing.assert_allclose(st, st[::-1, ::-1, ::-1], atol=1e-14)
+    assert st[2, 2, 2] > 0
+    # the stiffness annihilates constants on a full lattice: its stencil sums to zero
+    assert abs(st.sum()) < 1e-12
