@@ -38,6 +38,9 @@ typedef enum {
 const char* ngs_status_string(int status);
 const char* ngs_last_cuda_error(void);
 int ngs_version(void);
+/* Number of kernels this library has launched in the process (for launch accounting). */
+int64_t ngs_launch_count(void);
+void ngs_reset_launch_count(void);
 
 /* ======================================================================= hashing
  * ref: csrc/common/hashmap_cuda.cu:247-305 (hash_cuda), :204-235,307-339

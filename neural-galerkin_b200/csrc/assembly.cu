@@ -69,8 +69,8 @@ extern "C" int ngs_stencil_count(ngs_grid g, const int32_t* coords, int64_t V, u
                                  ngs_stream s) {
   if (!g.words || V < 0 || (V > 0 && (!coords || !masks || !counts))) return NGS_ERR_INVALID_ARG;
   if (V == 0) return NGS_OK;
-  stencil_count_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(g, coords, V, reinterpret_cast<uint4*>(masks),
-                                                                       counts);
+  { ngs_count_launch(); stencil_count_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(g, coords, V, reinterpret_cast<uint4*>(masks),
+                                                                       counts); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -81,8 +81,8 @@ extern "C" int ngs_stencil_fill(ngs_grid g, const int32_t* coords, int64_t V, co
   if (!g.words || V < 0 || (V > 0 && (!coords || !masks || !rowptr || !stencil125 || !cols || !vals || !diag_slot)))
     return NGS_ERR_INVALID_ARG;
   if (V == 0) return NGS_OK;
-  stencil_fill_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(
-      g, coords, V, reinterpret_cast<const uint4*>(masks), rowptr, stencil125, cols, vals, diag_slot);
+  { ngs_count_launch(); stencil_fill_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(
+      g, coords, V, reinterpret_cast<const uint4*>(masks), rowptr, stencil125, cols, vals, diag_slot); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -122,8 +122,8 @@ extern "C" int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n,
                                const int64_t* rowptr, double scale, double* vals, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rows || !phi || !masks || !rowptr || !vals))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  screen_gram_kernel<<<ngs_blocks(n * 32, 256), 256, 0, (cudaStream_t)s>>>(
-      rows, phi, n, w, reinterpret_cast<const uint4*>(masks), rowptr, scale, vals);
+  { ngs_count_launch(); screen_gram_kernel<<<ngs_blocks(n * 32, 256), 256, 0, (cudaStream_t)s>>>(
+      rows, phi, n, w, reinterpret_cast<const uint4*>(masks), rowptr, scale, vals); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -147,7 +147,7 @@ extern "C" int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, 
                               double* rhs, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rows || !phi || !rhs))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  screen_rhs_kernel<<<ngs_blocks(n * 27, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, w, nullptr, scale, rhs);
+  { ngs_count_launch(); screen_rhs_kernel<<<ngs_blocks(n * 27, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, w, nullptr, scale, rhs); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -156,7 +156,7 @@ extern "C" int ngs_correction_screen(const int32_t* rows, const float* phi, int6
                                      const float* field, double scale, double* rhs, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rows || !phi || !field || !rhs))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  screen_rhs_kernel<<<ngs_blocks(n * 27, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, w, field, -scale, rhs);
+  { ngs_count_launch(); screen_rhs_kernel<<<ngs_blocks(n * 27, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, w, field, -scale, rhs); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -248,13 +248,13 @@ extern "C" int ngs_rhs_normals(ngs_grid data_grid, const int32_t* data_coords, i
   if (tgt_grid.stride >= data_grid.stride) {
     if (n_data <= 0) return NGS_OK;
     if (!data_coords || !tgt_grid.words) return NGS_ERR_INVALID_ARG;
-    rhs_scatter_kernel<<<ngs_blocks(n_data, 128), 128, 0, st>>>(data_coords, n_data, data_grid.stride, normals,
-                                                               tgt_grid, tab_c, tab_g, tab_len, rhs);
+    { ngs_count_launch(); rhs_scatter_kernel<<<ngs_blocks(n_data, 128), 128, 0, st>>>(data_coords, n_data, data_grid.stride, normals,
+                                                               tgt_grid, tab_c, tab_g, tab_len, rhs); }
   } else {
     if (n_tgt <= 0) return NGS_OK;
     if (!tgt_coords || !data_grid.words) return NGS_ERR_INVALID_ARG;
-    rhs_gather_kernel<<<ngs_blocks(n_tgt, 128), 128, 0, st>>>(data_grid, normals, tgt_coords, n_tgt, tgt_grid.stride,
-                                                              tab_c, tab_g, tab_len, rhs);
+    { ngs_count_launch(); rhs_gather_kernel<<<ngs_blocks(n_tgt, 128), 128, 0, st>>>(data_grid, normals, tgt_coords, n_tgt, tgt_grid.stride,
+                                                              tab_c, tab_g, tab_len, rhs); }
   }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
@@ -310,8 +310,8 @@ extern "C" int ngs_correction_stiffness(const int32_t* fine_coords, int64_t n_fi
   if (n_fine < 0 || fine_stride <= 0 || cg.stride <= fine_stride || tab_len <= 0 || tab_len > 4096) return NGS_ERR_INVALID_ARG;
   if (n_fine == 0) return NGS_OK;
   if (!fine_coords || !cg.words || !x_coarse || !tab_c || !tab_g || !rhs) return NGS_ERR_INVALID_ARG;
-  correction_kernel<<<ngs_blocks(n_fine, 128), 128, 2 * tab_len * sizeof(double), (cudaStream_t)s>>>(
-      fine_coords, n_fine, fine_stride, cg, x_coarse, tab_c, tab_g, tab_len, rhs);
+  { ngs_count_launch(); correction_kernel<<<ngs_blocks(n_fine, 128), 128, 2 * tab_len * sizeof(double), (cudaStream_t)s>>>(
+      fine_coords, n_fine, fine_stride, cg, x_coarse, tab_c, tab_g, tab_len, rhs); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -328,8 +328,8 @@ extern "C" int ngs_finish_system(const double* vals64, int64_t nnz, const int64_
   if (nnz < 0 || V < 0 || (nnz > 0 && (!vals64 || !vals32)) || (V > 0 && (!diag_slot || !inv_diag)))
     return NGS_ERR_INVALID_ARG;
   if (nnz == 0 && V == 0) return NGS_OK;
-  finish_kernel<<<ngs_blocks(nnz > V ? nnz : V, 256), 256, 0, (cudaStream_t)s>>>(vals64, nnz, diag_slot, V, vals32,
-                                                                                inv_diag);
+  { ngs_count_launch(); finish_kernel<<<ngs_blocks(nnz > V ? nnz : V, 256), 256, 0, (cudaStream_t)s>>>(vals64, nnz, diag_slot, V, vals32,
+                                                                                inv_diag); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

@@ -92,7 +92,7 @@ extern "C" int ngs_grid_mark_points(ngs_grid g, const float* xyz, int64_t n, flo
                                     int max_level, ngs_stream s) {
   if (!grid_ok(g) || n < 0 || (n > 0 && !xyz)) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  mark_points_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, levels, max_level);
+  { ngs_count_launch(); mark_points_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, levels, max_level); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -102,8 +102,8 @@ extern "C" int ngs_grid_mark_coords(ngs_grid g, const int32_t* coords, int64_t n
   if (!grid_ok(g) || n < 0 || (n > 0 && !coords)) return NGS_ERR_INVALID_ARG;
   if (!offsets) n_off = 1;
   if (n == 0 || n_off <= 0) return NGS_OK;
-  mark_coords_kernel<<<ngs_blocks(n * n_off, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, offsets, n_off,
-                                                                             offset_scale);
+  { ngs_count_launch(); mark_coords_kernel<<<ngs_blocks(n * n_off, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, offsets, n_off,
+                                                                             offset_scale); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -118,7 +118,7 @@ extern "C" int ngs_grid_finalize(ngs_grid g, void* ws, size_t ws_bytes, int64_t*
 
 extern "C" int ngs_grid_emit_coords(ngs_grid g, int32_t* coords, ngs_stream s) {
   if (!grid_ok(g) || !coords) return NGS_ERR_INVALID_ARG;
-  emit_coords_kernel<<<ngs_blocks(g.nwords, 256), 256, 0, (cudaStream_t)s>>>(g, coords);
+  { ngs_count_launch(); emit_coords_kernel<<<ngs_blocks(g.nwords, 256), 256, 0, (cudaStream_t)s>>>(g, coords); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -126,7 +126,7 @@ extern "C" int ngs_grid_emit_coords(ngs_grid g, int32_t* coords, ngs_stream s) {
 extern "C" int ngs_grid_lookup(ngs_grid g, const int32_t* coords, int64_t n, int64_t* rows, ngs_stream s) {
   if (!grid_ok(g) || n < 0 || (n > 0 && (!coords || !rows))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  lookup_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, rows);
+  { ngs_count_launch(); lookup_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, rows); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -182,8 +182,8 @@ extern "C" int ngs_splat_weights(ngs_grid g, const float* xyz, int64_t n, float 
                                  ngs_stream s) {
   if (!grid_ok(g) || n < 0 || (n > 0 && (!xyz || !wd))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  splat_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, nullptr, 1, nullptr,
-                                                                 nullptr, 0, 1.f, wd);
+  { ngs_count_launch(); splat_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, nullptr, 1, nullptr,
+                                                                 nullptr, 0, 1.f, wd); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -193,8 +193,8 @@ extern "C" int ngs_splat_data(ngs_grid g, const float* xyz, int64_t n, float inv
                               float* out, ngs_stream s) {
   if (!grid_ok(g) || n < 0 || dim < 1 || (n > 0 && (!xyz || !out))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  splat_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, data, dim, point_scale,
-                                                                 levels, level, scale, out);
+  { ngs_count_launch(); splat_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, data, dim, point_scale,
+                                                                 levels, level, scale, out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -261,8 +261,8 @@ extern "C" int ngs_density_eval(ngs_grid g, const float* xyz, int64_t n, float i
   if (n == 0) return NGS_OK;
   const float inv_md = 1.0f / min_density;
   const float inv_ln4 = 1.0f / (float)1.3862943611198906;
-  density_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, wd, inv_md, inv_ln4, depth,
-                                                                   density, levels, weight);
+  { ngs_count_launch(); density_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, wd, inv_md, inv_ln4, depth,
+                                                                   density, levels, weight); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -294,7 +294,7 @@ extern "C" int ngs_point_basis(ngs_grid g, const float* xyz, int64_t n, float in
                                float* phi, ngs_stream s) {
   if (!grid_ok(g) || n < 0 || (n > 0 && (!xyz || !rows || !phi))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  point_basis_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, rows, phi);
+  { ngs_count_launch(); point_basis_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(g, xyz, n, inv_vs, vs, rows, phi); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -316,7 +316,7 @@ extern "C" int ngs_point_field(const int32_t* rows, const float* phi, int64_t n,
                                int accumulate, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rows || !phi || !x || !out))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  point_field_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, x, out, accumulate);
+  { ngs_count_launch(); point_field_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(rows, phi, n, x, out, accumulate); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -366,7 +366,7 @@ extern "C" int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv
                               int grad, float* out, ngs_stream s) {
   if (!grid_ok(g) || n < 0 || (n > 0 && (!pos || !x || !out))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  eval_field_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(g, pos, n, inv_vs, vs, x, grad, out);
+  { ngs_count_launch(); eval_field_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(g, pos, n, inv_vs, vs, x, grad, out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

@@ -36,13 +36,15 @@ extern "C" int ngs_hash_coords(const void* coords, int coords_int64, int64_t n, 
   if (n == 0) return NGS_OK;
   cudaStream_t st = (cudaStream_t)s;
   const unsigned b = ngs_blocks(n, 256);
-#define NGS_HASH_CASE(T, D) hash_rows_kernel<T, D><<<b, 256, 0, st>>>((const T*)coords, n, out)
-  if (coords_int64) {
-    if (dim == 2) NGS_HASH_CASE(int64_t, 2); else if (dim == 3) NGS_HASH_CASE(int64_t, 3); else NGS_HASH_CASE(int64_t, 4);
-  } else {
-    if (dim == 2) NGS_HASH_CASE(int32_t, 2); else if (dim == 3) NGS_HASH_CASE(int32_t, 3); else NGS_HASH_CASE(int32_t, 4);
+  const int key = (coords_int64 ? 10 : 0) + dim;
+  switch (key) {
+    case 2: { ngs_count_launch(); hash_rows_kernel<int32_t, 2><<<b, 256, 0, st>>>((const int32_t*)coords, n, out); } break;
+    case 3: { ngs_count_launch(); hash_rows_kernel<int32_t, 3><<<b, 256, 0, st>>>((const int32_t*)coords, n, out); } break;
+    case 4: { ngs_count_launch(); hash_rows_kernel<int32_t, 4><<<b, 256, 0, st>>>((const int32_t*)coords, n, out); } break;
+    case 12: { ngs_count_launch(); hash_rows_kernel<int64_t, 2><<<b, 256, 0, st>>>((const int64_t*)coords, n, out); } break;
+    case 13: { ngs_count_launch(); hash_rows_kernel<int64_t, 3><<<b, 256, 0, st>>>((const int64_t*)coords, n, out); } break;
+    default: { ngs_count_launch(); hash_rows_kernel<int64_t, 4><<<b, 256, 0, st>>>((const int64_t*)coords, n, out); } break;
   }
-#undef NGS_HASH_CASE
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -55,11 +57,11 @@ extern "C" int ngs_kernel_hash(const void* coords, int coords_int64, int64_t n, 
   cudaStream_t st = (cudaStream_t)s;
   const unsigned b = ngs_blocks(n * k, 256);
   if (coords_int64) {
-    if (dim == 3) kernel_hash_kernel<int64_t, 3><<<b, 256, 0, st>>>((const int64_t*)coords, n, offsets, k, out);
-    else kernel_hash_kernel<int64_t, 4><<<b, 256, 0, st>>>((const int64_t*)coords, n, offsets, k, out);
+    if (dim == 3) { ngs_count_launch(); kernel_hash_kernel<int64_t, 3><<<b, 256, 0, st>>>((const int64_t*)coords, n, offsets, k, out); }
+    else { ngs_count_launch(); kernel_hash_kernel<int64_t, 4><<<b, 256, 0, st>>>((const int64_t*)coords, n, offsets, k, out); }
   } else {
-    if (dim == 3) kernel_hash_kernel<int32_t, 3><<<b, 256, 0, st>>>((const int32_t*)coords, n, offsets, k, out);
-    else kernel_hash_kernel<int32_t, 4><<<b, 256, 0, st>>>((const int32_t*)coords, n, offsets, k, out);
+    if (dim == 3) { ngs_count_launch(); kernel_hash_kernel<int32_t, 3><<<b, 256, 0, st>>>((const int32_t*)coords, n, offsets, k, out); }
+    else { ngs_count_launch(); kernel_hash_kernel<int32_t, 4><<<b, 256, 0, st>>>((const int32_t*)coords, n, offsets, k, out); }
   }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
@@ -167,8 +169,8 @@ extern "C" int ngs_hash_table_build(ngs_hash_table* t, const int64_t* keys, cons
   if ((reinterpret_cast<uintptr_t>(t->slots) & 15u) != 0) return NGS_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)s;
   Slot* slots = static_cast<Slot*>(t->slots);
-  table_init_kernel<<<ngs_blocks(t->nslots, 256), 256, 0, st>>>(slots, t->nslots);
-  if (n > 0) table_insert_kernel<<<ngs_blocks(n, 256), 256, 0, st>>>(slots, t->nslots - 1, keys, vals, n, status_dev);
+  { ngs_count_launch(); table_init_kernel<<<ngs_blocks(t->nslots, 256), 256, 0, st>>>(slots, t->nslots); }
+  if (n > 0) { ngs_count_launch(); table_insert_kernel<<<ngs_blocks(n, 256), 256, 0, st>>>(slots, t->nslots - 1, keys, vals, n, status_dev); }
   t->inserted = n;
   NGS_CHECK_LAUNCH();
   return NGS_OK;
@@ -178,8 +180,8 @@ extern "C" int ngs_hash_table_query(const ngs_hash_table* t, const int64_t* keys
                                     ngs_stream s) {
   if (!t || !t->slots || m < 0 || (m > 0 && (!keys || !out))) return NGS_ERR_INVALID_ARG;
   if (m == 0) return NGS_OK;
-  table_query_kernel<<<ngs_blocks(m * 8, 256), 256, 0, (cudaStream_t)s>>>(
-      static_cast<const Slot*>(t->slots), t->nslots - 1, keys, m, out);
+  { ngs_count_launch(); table_query_kernel<<<ngs_blocks(m * 8, 256), 256, 0, (cudaStream_t)s>>>(
+      static_cast<const Slot*>(t->slots), t->nslots - 1, keys, m, out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -188,8 +190,8 @@ extern "C" int ngs_hash_table_query_coords(const ngs_hash_table* t, const int32_
                                            ngs_stream s) {
   if (!t || !t->slots || m < 0 || (m > 0 && (!coords || !out))) return NGS_ERR_INVALID_ARG;
   if (m == 0) return NGS_OK;
-  table_query_coords_kernel<<<ngs_blocks(m * 8, 256), 256, 0, (cudaStream_t)s>>>(
-      static_cast<const Slot*>(t->slots), t->nslots - 1, coords, m, out);
+  { ngs_count_launch(); table_query_coords_kernel<<<ngs_blocks(m * 8, 256), 256, 0, (cudaStream_t)s>>>(
+      static_cast<const Slot*>(t->slots), t->nslots - 1, coords, m, out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

@@ -130,8 +130,8 @@ extern "C" int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_bas
     return NGS_ERR_INVALID_ARG;
   if (n_primal == 0) return NGS_OK;
   const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
-  dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
-      GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, cnt);
+  { ngs_count_launch(); dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
+      GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, cnt); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -143,9 +143,9 @@ extern "C" int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_
     return NGS_ERR_INVALID_ARG;
   if (n_primal == 0) return NGS_OK;
   const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
-  dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
+  { ngs_count_launch(); dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
       KeyLookup{static_cast<const Slot*>(dual->slots), dual->nslots - 1}, primal_base, n_primal, stride, depth,
-      idx_base, acc, cnt);
+      idx_base, acc, cnt); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -168,7 +168,7 @@ __global__ void compact_acc_kernel(const int32_t* __restrict__ acc, const int32_
 extern "C" int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, ngs_stream s) {
   if (n < 0 || (n > 0 && (!cnt || !keep))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  select_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(cnt, n, keep);
+  { ngs_count_launch(); select_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(cnt, n, keep); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -178,7 +178,7 @@ extern "C" int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, cons
   if (n < 0 || (n > 0 && (!acc || !keep || !keep_offset || !acc_out))) return NGS_ERR_INVALID_ARG;
   if ((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(acc_out)) & 15u) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  compact_acc_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(acc, keep, keep_offset, n, acc_out);
+  { ngs_count_launch(); compact_acc_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(acc, keep, keep_offset, n, acc_out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -228,7 +228,7 @@ extern "C" int ngs_dual_mc_count(const int32_t* acc, int64_t n_cubes, const floa
                                  ngs_stream s) {
   if (n_cubes < 0 || (n_cubes > 0 && (!acc || !values || !vcount))) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, n_cubes, values, vcount);
+  { ngs_count_launch(); dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, n_cubes, values, vcount); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -238,8 +238,8 @@ extern "C" int ngs_dual_mc_emit(const int32_t* acc, int64_t n_cubes, const float
   if (n_cubes < 0 || (n_cubes > 0 && (!acc || !pos || !values || !voffset || !tris || !vert_ids)))
     return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, n_cubes, pos, values, voffset, tris,
-                                                                        vert_ids);
+  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, n_cubes, pos, values, voffset, tris,
+                                                                        vert_ids); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -305,7 +305,7 @@ extern "C" int ngs_vdedup_count(const int32_t* vert_ids, int64_t n_keys, int32_t
   if (n_keys < 0 || (n_keys > 0 && (!vert_ids || !bucket_count))) return NGS_ERR_INVALID_ARG;
   if (n_keys == 0) return NGS_OK;
   if (n_keys > 0x7fffffffLL) return NGS_ERR_INVALID_ARG;
-  vd_count_kernel<<<ngs_blocks(n_keys, 256), 256, 0, (cudaStream_t)s>>>(vert_ids, n_keys, bucket_count);
+  { ngs_count_launch(); vd_count_kernel<<<ngs_blocks(n_keys, 256), 256, 0, (cudaStream_t)s>>>(vert_ids, n_keys, bucket_count); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -316,8 +316,8 @@ extern "C" int ngs_vdedup_sort(const int32_t* vert_ids, int64_t n_keys, const in
     return NGS_ERR_INVALID_ARG;
   if (n_keys == 0) return NGS_OK;
   cudaStream_t st = (cudaStream_t)s;
-  vd_scatter_kernel<<<ngs_blocks(n_keys, 256), 256, 0, st>>>(vert_ids, n_keys, bucket_start, bucket_fill, sorted_keys);
-  vd_sort_kernel<<<ngs_blocks(n_buckets, 128), 128, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first);
+  { ngs_count_launch(); vd_scatter_kernel<<<ngs_blocks(n_keys, 256), 256, 0, st>>>(vert_ids, n_keys, bucket_start, bucket_fill, sorted_keys); }
+  { ngs_count_launch(); vd_sort_kernel<<<ngs_blocks(n_buckets, 128), 128, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -329,9 +329,9 @@ extern "C" int ngs_vdedup_emit(const int32_t* vert_ids, const float* tris, int64
                                     !vertex_id || !faces || !vertices)))
     return NGS_ERR_INVALID_ARG;
   if (n_keys == 0) return NGS_OK;
-  vd_emit_kernel<<<ngs_blocks(n_keys, 256), 256, 0, (cudaStream_t)s>>>(vert_ids, tris, n_keys, bucket_start,
+  { ngs_count_launch(); vd_emit_kernel<<<ngs_blocks(n_keys, 256), 256, 0, (cudaStream_t)s>>>(vert_ids, tris, n_keys, bucket_start,
                                                                      bucket_count, sorted_keys, vertex_id, faces,
-                                                                     vertices);
+                                                                     vertices); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -385,7 +385,7 @@ extern "C" int ngs_conformal_children(const int32_t* parents, int64_t n_parents,
                                       ngs_stream s) {
   if (n_parents < 0 || (n_parents > 0 && (!parents || !children))) return NGS_ERR_INVALID_ARG;
   if (n_parents == 0) return NGS_OK;
-  children_kernel<<<ngs_blocks(n_parents * 8, 256), 256, 0, (cudaStream_t)s>>>(parents, n_parents, stride, children);
+  { ngs_count_launch(); children_kernel<<<ngs_blocks(n_parents * 8, 256), 256, 0, (cudaStream_t)s>>>(parents, n_parents, stride, children); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -393,7 +393,7 @@ extern "C" int ngs_conformal_children(const int32_t* parents, int64_t n_parents,
 extern "C" int ngs_leaf_flags(const int32_t* cells, int64_t n, ngs_grid finer_parents, int32_t* leaf, ngs_stream s) {
   if (n < 0 || (n > 0 && (!cells || !leaf))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  leaf_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(cells, n, finer_parents, leaf);
+  { ngs_count_launch(); leaf_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(cells, n, finer_parents, leaf); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -402,7 +402,7 @@ extern "C" int ngs_compact_coords(const int32_t* coords, const int32_t* keep, co
                                   int32_t* out, ngs_stream s) {
   if (n < 0 || (n > 0 && (!coords || !keep || !keep_offset || !out))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  compact_coords_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(coords, keep, keep_offset, n, out);
+  { ngs_count_launch(); compact_coords_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(coords, keep, keep_offset, n, out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -411,8 +411,8 @@ extern "C" int ngs_expand_cells(const int32_t* cells, int64_t n, int n_up, int s
                                 float* pos, ngs_stream s) {
   if (n < 0 || n_up < 1 || (n > 0 && (!cells || !out))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  expand_kernel<<<ngs_blocks(n * n_up * n_up * n_up, 256), 256, 0, (cudaStream_t)s>>>(cells, n, n_up, stride, evs, out,
-                                                                                     pos);
+  { ngs_count_launch(); expand_kernel<<<ngs_blocks(n * n_up * n_up * n_up, 256), 256, 0, (cudaStream_t)s>>>(cells, n, n_up, stride, evs, out,
+                                                                                     pos); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

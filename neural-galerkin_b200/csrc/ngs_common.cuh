@@ -106,52 +106,6 @@ NGS_DEV T warp_sum(T v) {
   return v;
 }
 
-// Bounded grid-wide barrier for persistent kernels launched cooperatively
-// (all blocks co-resident).  The last block to arrive may run `on_last`
-// (e.g. a fixed-order reduction of per-block partials) before releasing the
-// others.  Waits give up after `limit_cycles` clock cycles: the flag
-// `*error` is set and the barrier returns false so the kernel can exit.
-struct GridBarrier {
-  unsigned int* count;
-  unsigned int* generation;
-  int* error;
-  unsigned int nblocks;
-  long long limit_cycles;
-};
-
-template <typename F>
-NGS_DEV bool grid_barrier(const GridBarrier& gb, F on_last) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    volatile unsigned int* gen = gb.generation;
-    const unsigned int g = *gen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(gb.count, 1u);
-    if (arrived == gb.nblocks - 1) {
-      *gb.count = 0;
-      on_last();
-      __threadfence();
-      atomicExch(gb.generation, g + 1u);
-    } else {
-      const long long t0 = clock64();
-      while (*gen == g) {
-        if (*(volatile int*)gb.error) { ok = 0; break; }
-        if (clock64() - t0 > gb.limit_cycles) {
-          atomicExch(gb.error, NGS_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-      __threadfence();
-    }
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
 #define NGS_CHECK_LAUNCH()                                  \
   do {                                                      \
     cudaError_t _e = cudaGetLastError();                    \
@@ -159,6 +113,8 @@ NGS_DEV bool grid_barrier(const GridBarrier& gb, F on_last) {
   } while (0)
 
 int ngs_set_cuda_error(cudaError_t e);
+// Host-side count of kernel launches issued by the library (every <<<>>> and cooperative launch).
+void ngs_count_launch();
 
 NGS_DEV int64_t ngs_gtid() { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
 NGS_DEV int64_t ngs_gstride() { return (int64_t)gridDim.x * blockDim.x; }

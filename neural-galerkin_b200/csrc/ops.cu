@@ -26,8 +26,8 @@ extern "C" int ngs_sparse_meshgrid(const int64_t* a_start, const int64_t* a_len,
   if (n_points < 0 || (n_points > 0 && (!a_start || !a_len || !b_start || !b_len || !ab_start || !a_inds || !b_inds)))
     return NGS_ERR_INVALID_ARG;
   if (n_points == 0) return NGS_OK;
-  meshgrid_kernel<<<ngs_blocks(n_points * 32, 256), 256, 0, (cudaStream_t)s>>>(a_start, a_len, b_start, b_len,
-                                                                              ab_start, n_points, a_inds, b_inds);
+  { ngs_count_launch(); meshgrid_kernel<<<ngs_blocks(n_points * 32, 256), 256, 0, (cudaStream_t)s>>>(a_start, a_len, b_start, b_len,
+                                                                              ab_start, n_points, a_inds, b_inds); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -104,9 +104,9 @@ extern "C" int ngs_screened_multiplication(const ngs_hash_table* pairs, const fl
   if (n_points == 0) return NGS_OK;
   if (!a_val || !b_val || !a_inds || !b_inds || !a_start || !a_len || !b_start || !b_len || !weight || !res)
     return NGS_ERR_INVALID_ARG;
-  smult_kernel<<<ngs_blocks(n_points * 32, 256), 256, 0, (cudaStream_t)s>>>(
+  { ngs_count_launch(); smult_kernel<<<ngs_blocks(n_points * 32, 256), 256, 0, (cudaStream_t)s>>>(
       static_cast<const Slot*>(pairs->slots), pairs->nslots - 1, a_val, b_val, val_dim, a_inds, b_inds, a_start, a_len,
-      b_start, b_len, weight, n_points, res);
+      b_start, b_len, weight, n_points, res); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -122,9 +122,9 @@ extern "C" int ngs_screened_multiplication_backward(const ngs_hash_table* pairs,
   if (!a_val || !b_val || !a_inds || !b_inds || !a_start || !a_len || !b_start || !b_len || !weight || !grad_res ||
       !grad_a || !grad_b || !grad_w)
     return NGS_ERR_INVALID_ARG;
-  smult_back_kernel<<<ngs_blocks(n_points * 32, 256), 256, 0, (cudaStream_t)s>>>(
+  { ngs_count_launch(); smult_back_kernel<<<ngs_blocks(n_points * 32, 256), 256, 0, (cudaStream_t)s>>>(
       static_cast<const Slot*>(pairs->slots), pairs->nslots - 1, a_val, b_val, val_dim, a_inds, b_inds, a_start, a_len,
-      b_start, b_len, weight, n_points, grad_res, grad_a, grad_b, grad_w);
+      b_start, b_len, weight, n_points, grad_res, grad_a, grad_b, grad_w); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -200,8 +200,8 @@ extern "C" int ngs_ddi_forward(const float* src, const float* tgt, const int64_t
   if (n_pairs < 0 || C < 1 || C > 32 || R < 1) return NGS_ERR_INVALID_ARG;
   if (n_pairs == 0) return NGS_OK;
   if (!src || !tgt || !rel_pos || !ff || !dfdf || !p || !q) return NGS_ERR_INVALID_ARG;
-  ddi_fwd_kernel<32><<<ngs_blocks(n_pairs * 3, 128), 128, 0, (cudaStream_t)s>>>(src, tgt, rel_pos, ff, dfdf, n_pairs,
-                                                                              C, R, p, q);
+  { ngs_count_launch(); ddi_fwd_kernel<32><<<ngs_blocks(n_pairs * 3, 128), 128, 0, (cudaStream_t)s>>>(src, tgt, rel_pos, ff, dfdf, n_pairs,
+                                                                              C, R, p, q); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -213,8 +213,8 @@ extern "C" int ngs_ddi_backward(const float* src, const float* tgt, const int64_
   if (n_pairs == 0) return NGS_OK;
   if (!src || !tgt || !rel_pos || !ff || !dfdf || !grad_p || !grad_q || !grad_src || !grad_tgt)
     return NGS_ERR_INVALID_ARG;
-  ddi_bwd_kernel<32><<<ngs_blocks(n_pairs * 3, 128), 128, 0, (cudaStream_t)s>>>(src, tgt, rel_pos, ff, dfdf, grad_p,
-                                                                              grad_q, n_pairs, C, R, grad_src, grad_tgt);
+  { ngs_count_launch(); ddi_bwd_kernel<32><<<ngs_blocks(n_pairs * 3, 128), 128, 0, (cudaStream_t)s>>>(src, tgt, rel_pos, ff, dfdf, grad_p,
+                                                                              grad_q, n_pairs, C, R, grad_src, grad_tgt); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -312,7 +312,7 @@ __global__ void primal_emit_kernel(const float* __restrict__ base, const float* 
 extern "C" int ngs_primal_mc_count(const float* sdf, int64_t n_cubes, int r, int32_t* vcount, ngs_stream s) {
   if (n_cubes < 0 || r < 1 || (n_cubes > 0 && (!sdf || !vcount))) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  primal_count_kernel<<<ngs_blocks(n_cubes * r * r * r, 256), 256, 0, (cudaStream_t)s>>>(sdf, n_cubes, r, vcount);
+  { ngs_count_launch(); primal_count_kernel<<<ngs_blocks(n_cubes * r * r * r, 256), 256, 0, (cudaStream_t)s>>>(sdf, n_cubes, r, vcount); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -322,8 +322,8 @@ extern "C" int ngs_primal_mc_emit(const float* base, const float* sdf, int64_t n
   if (n_cubes < 0 || r < 1) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
   if (!base || !sdf || !voffset || !tris || !vert_ids || !src_ids || !src_w) return NGS_ERR_INVALID_ARG;
-  primal_emit_kernel<<<ngs_blocks(n_cubes * r * r * r, 128), 128, 0, (cudaStream_t)s>>>(base, sdf, n_cubes, r, voffset,
-                                                                                       tris, vert_ids, src_ids, src_w);
+  { ngs_count_launch(); primal_emit_kernel<<<ngs_blocks(n_cubes * r * r * r, 128), 128, 0, (cudaStream_t)s>>>(base, sdf, n_cubes, r, voffset,
+                                                                                       tris, vert_ids, src_ids, src_w); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

@@ -10,8 +10,18 @@
 //     phase B  (own rows)  w = A u, partial dots (r,u), (w,u), (r,r)
 //     barrier + reduce     the last block to arrive sums the per-block partials in
 //                          block order (deterministic) and releases the others.
-// Every wait is bounded (clock64); on timeout the kernel records NGS_ERR_TIMEOUT
-// and returns.  Dots are FP64 in every mode.
+// Every wait is bounded by the global nanosecond timer; on timeout the kernel
+// records NGS_ERR_TIMEOUT and returns.  Every solve is bounded too: at most
+// NGS_PCG_ITER_CAP iterations, and a deadline that the last block of each
+// reduction checks, so that all blocks stop at the same iteration.  Dots are
+// FP64 in every mode.
+//
+// Mixed precision (NGS_PCG_MIXED) is iterative refinement: the inner PCG runs on
+// the FP32 matrix values with FP64 vectors and FP64 accumulation, until its
+// residual has dropped by `inner_rtol`; then the true residual b - A x is formed
+// with the FP64 matrix and the inner solve restarts from it.  The FP32 matrix is
+// a fixed SPD perturbation of the FP64 one, so each outer step contracts the
+// error by about |A32 - A64| |A64^-1| and the solve converges to the FP64 system.
 #include <cmath>
 #include "ngs_common.cuh"
 
@@ -43,9 +53,20 @@ struct PcgArgs {
   double tol;
   int max_iter;
   int replace_every;         // <= 0: never
-  long long limit_cycles;
+  double inner_rtol;          // MIXED: relative reduction of an inner solve
+  unsigned long long wait_ns;     // bound of one barrier wait
+  unsigned long long* deadline;   // absolute global-timer deadline, set at the first reduction
+  unsigned long long budget_ns;   // time budget of the whole solve
   unsigned int nblocks;
 };
+
+constexpr int NGS_PCG_ITER_CAP = 20000;
+
+NGS_DEV unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 template <typename T>
 NGS_DEV T ld_cg(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
@@ -94,15 +115,18 @@ NGS_DEV bool reduce_barrier(const PcgArgs& a, const double (&v)[NV], double (&ou
         for (int i = 0; i < PCG_THREADS / 32; i++) t += red[k][i];
         a.result[k] = t;
       }
+      const unsigned long long now = global_ns();
+      if (*a.deadline == 0ull) *a.deadline = now + a.budget_ns;
+      a.result[3] = now > *a.deadline ? 1.0 : 0.0;   // one decision for every block
       *a.count = 0;
       __threadfence();
       atomicExch(a.gen, gen0 + 1u);
     }
   } else if (threadIdx.x == 0) {
-    const long long t0 = clock64();
+    const unsigned long long t0 = global_ns();
     while (*reinterpret_cast<volatile unsigned int*>(a.gen) == gen0) {
       if (*reinterpret_cast<volatile int*>(a.error)) { ok = 0; break; }
-      if (clock64() - t0 > a.limit_cycles) {
+      if (global_ns() - t0 > a.wait_ns) {
         atomicExch(a.error, NGS_ERR_TIMEOUT);
         ok = 0;
         break;
@@ -116,6 +140,8 @@ NGS_DEV bool reduce_barrier(const PcgArgs& a, const double (&v)[NV], double (&ou
   for (int k = 0; k < NV; k++) out[k] = ld_cg(a.result + k);
   return ok != 0;
 }
+
+NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0; }
 
 NGS_DEV bool plain_barrier(const PcgArgs& a) {
   double v[1] = {0.0}, o[1];
@@ -150,13 +176,15 @@ NGS_DEV double spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT
 template <int MODE>
 struct PcgTypes;
 template <> struct PcgTypes<NGS_PCG_REFERENCE> { using MT = float; using VT = float; using RT = float; };
-template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = float; using RT = double; };
+template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = double; using RT = double; };
 template <> struct PcgTypes<NGS_PCG_FP64> { using MT = double; using VT = double; using RT = double; };
 
-// Recurrence SpMV of a mode: FP32 matrix with FP32 accumulation, or all FP64.
+// Recurrence SpMV of a mode: REFERENCE is all FP32 (as cuSPARSE SpMV in the reference);
+// MIXED reads FP32 matrix values and accumulates in FP64; FP64 is all FP64.
 template <int MODE, typename VT, typename Epi>
 NGS_DEV double spmv_mode(const PcgArgs& a, const VT* v, Epi epi) {
   if constexpr (MODE == NGS_PCG_FP64) return spmv_rows<double, VT, double>(a, static_cast<const double*>(a.vals), v, epi);
+  else if constexpr (MODE == NGS_PCG_MIXED) return spmv_rows<float, VT, double>(a, static_cast<const float*>(a.vals), v, epi);
   else return spmv_rows<float, VT, float>(a, static_cast<const float*>(a.vals), v, epi);
 }
 
@@ -212,9 +240,12 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
   double gamma = res[0], delta = res[1], rho = res[2];
   double alpha = delta != 0.0 ? gamma / delta : 0.0, beta = 0.0;
   int it = 0, replacements = 0;
-  bool converged = sqrt(rho) <= atol || bnorm == 0.0;
-  const bool bounded = a.max_iter >= 0;
-  while (!converged && (!bounded || it < a.max_iter)) {
+  const double rtol_inner = MODE == NGS_PCG_MIXED ? a.inner_rtol : 0.0;
+  double target = fmax(atol, rtol_inner * sqrt(rho));
+  bool converged = sqrt(rho) <= atol || bnorm == 0.0, timed_out = false;
+  const int cap = (a.max_iter >= 0 && a.max_iter < NGS_PCG_ITER_CAP) ? a.max_iter : NGS_PCG_ITER_CAP;
+  while (!converged && it < cap) {
+    if (past_deadline(a)) { timed_out = true; break; }
     const bool replace =
         (MODE == NGS_PCG_MIXED && a.replace_every > 0 && (it + 1) % a.replace_every == 0) ||
         (MODE == NGS_PCG_REFERENCE && a.replace_every > 0 && (it + 1) % sqrt_n == 0);
@@ -251,28 +282,25 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
     const double gamma_new = res[0];
     delta = res[1];
     rho = res[2];
-    if (sqrt(rho) <= atol) {
-      if (MODE == NGS_PCG_MIXED && !replace) {
-        // final FP64 refinement check: the recursive residual says converged -- confirm it
-        // with the true residual; if it is not there yet, restart from the true residual.
-        if (!plain_barrier(a)) return;
-        part[0] = part[1] = part[2] = 0.0;
-        part[2] = spmv_rows<double, RT, double>(a, a.vals64, x, true_res_epi);
-        replacements++;
-        if (!plain_barrier(a)) return;
-        part[1] = spmv_mode<MODE>(a, u, w_epi);
-        for (int64_t i = t0; i < n; i += ts) part[0] += (double)r[i] * (double)u[i];
-        if (!reduce_barrier<3>(a, part, res)) return;
-        rho = res[2];
-        if (sqrt(rho) <= atol) { converged = true; break; }
-        gamma = res[0];
-        delta = res[1];
-        alpha = delta != 0.0 ? gamma / delta : 0.0;
-        beta = 0.0;
-        continue;
-      }
-      converged = true;
-      break;
+    if (sqrt(rho) <= target) {
+      if (MODE != NGS_PCG_MIXED) { converged = true; break; }
+      // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
+      if (!plain_barrier(a)) return;
+      part[0] = part[1] = part[2] = 0.0;
+      part[2] = spmv_rows<double, RT, double>(a, a.vals64, x, true_res_epi);
+      replacements++;
+      if (!plain_barrier(a)) return;
+      part[1] = spmv_mode<MODE>(a, u, w_epi);
+      for (int64_t i = t0; i < n; i += ts) part[0] += (double)r[i] * (double)u[i];
+      if (!reduce_barrier<3>(a, part, res)) return;
+      rho = res[2];
+      if (sqrt(rho) <= atol) { converged = true; break; }
+      gamma = res[0];
+      delta = res[1];
+      alpha = delta != 0.0 ? gamma / delta : 0.0;
+      beta = 0.0;
+      target = fmax(atol, rtol_inner * sqrt(rho));
+      continue;
     }
     beta = gamma != 0.0 ? gamma_new / gamma : 0.0;
     const double den = delta - beta * gamma_new / alpha;
@@ -283,7 +311,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
     for (int64_t i = t0; i < n; i += ts) a.x32_out[i] = (float)x[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.info[0] = it;
-    a.info[1] = converged ? NGS_OK : NGS_ERR_NOT_CONVERGED;
+    a.info[1] = converged ? NGS_OK : (timed_out ? NGS_ERR_TIMEOUT : NGS_ERR_NOT_CONVERGED);
     a.info[2] = replacements;
     a.resid[0] = sqrt(rho);
     a.resid[1] = bnorm;
@@ -293,20 +321,19 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
-  const size_t vt = mode == NGS_PCG_FP64 ? 8 : 4;
+  const size_t vt = mode == NGS_PCG_REFERENCE ? 4 : 8;
   const size_t rt = mode == NGS_PCG_REFERENCE ? 4 : 8;
   size_t bytes = align_up(n * rt) + 4 * align_up(n * vt);     // r, p, s, u, w
   bytes += align_up((size_t)148 * 32 * 4 * sizeof(double));    // partials (upper bound of blocks)
-  bytes += align_up(4 * sizeof(double)) + align_up(4 * sizeof(unsigned int));
+  bytes += align_up(4 * sizeof(double)) + align_up(8 * sizeof(unsigned int));
   return bytes;
 }
 
 template <int MODE>
 static int launch_pcg(PcgArgs& a, int blocks_req, cudaStream_t st) {
-  int dev = 0, sms = 0, per_sm = 0, clock_khz = 0;
+  int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, 0);
   if (per_sm < 1) return NGS_ERR_CUDA;
   int64_t blocks = (int64_t)sms * per_sm;
@@ -316,6 +343,7 @@ static int launch_pcg(PcgArgs& a, int blocks_req, cudaStream_t st) {
   if (blocks > 148 * 32) blocks = 148 * 32;
   a.nblocks = (unsigned int)blocks;
   void* args[] = {&a};
+  ngs_count_launch();
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)pcg_kernel<MODE>, dim3((unsigned)blocks), dim3(PCG_THREADS),
                                               args, 0, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
@@ -340,7 +368,7 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
     cudaMemsetAsync(resid_dev, 0, 2 * sizeof(double), st);
     return NGS_OK;
   }
-  const size_t vt = mode == NGS_PCG_FP64 ? 8 : 4;
+  const size_t vt = mode == NGS_PCG_REFERENCE ? 4 : 8;
   const size_t rt = mode == NGS_PCG_REFERENCE ? 4 : 8;
   char* base = static_cast<char*>(ws);
   PcgArgs a{};
@@ -364,17 +392,17 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   a.count = ctl;
   a.gen = ctl + 1;
   a.error = reinterpret_cast<int*>(ctl + 2);
-  cudaMemsetAsync(ctl, 0, 4 * sizeof(unsigned int), st);
+  a.deadline = reinterpret_cast<unsigned long long*>(ctl + 4);
+  cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned int), st);
   a.info = info_dev;
   a.resid = resid_dev;
   a.tol = cfg->tol;
   a.max_iter = cfg->max_iter;
   a.replace_every = mode == NGS_PCG_REFERENCE ? (cfg->res_fix ? 1 : 0) : cfg->replace_every;
-  int dev = 0, clock_khz = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, dev);
   const double timeout = cfg->timeout_s > 0 ? cfg->timeout_s : 10.0;
-  a.limit_cycles = (long long)(timeout * (double)clock_khz * 1000.0 * 1.2);
+  a.wait_ns = (unsigned long long)(timeout * 1e9);
+  a.budget_ns = a.wait_ns;
+  a.inner_rtol = 1.0e-4;
   int rc;
   if (mode == NGS_PCG_REFERENCE) rc = launch_pcg<NGS_PCG_REFERENCE>(a, cfg->blocks, st);
   else if (mode == NGS_PCG_MIXED) rc = launch_pcg<NGS_PCG_MIXED>(a, cfg->blocks, st);
@@ -419,7 +447,7 @@ extern "C" int ngs_spmv64(int64_t n, const int64_t* rowptr, const int32_t* cols,
                           double* y, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rowptr || !cols || !vals || !x || !y))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  spmv64_kernel<<<ngs_blocks(n * 16, 256), 256, 0, (cudaStream_t)s>>>(n, rowptr, cols, vals, x, y);
+  { ngs_count_launch(); spmv64_kernel<<<ngs_blocks(n * 16, 256), 256, 0, (cudaStream_t)s>>>(n, rowptr, cols, vals, x, y); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -427,7 +455,7 @@ extern "C" int ngs_spmv64(int64_t n, const int64_t* rowptr, const int32_t* cols,
 extern "C" int ngs_dot64(const double* a, const double* b, int64_t n, double* out_dev, ngs_stream s) {
   if (n < 0 || !out_dev || (n > 0 && (!a || !b))) return NGS_ERR_INVALID_ARG;
   cudaMemsetAsync(out_dev, 0, sizeof(double), (cudaStream_t)s);
-  if (n > 0) dot64_kernel<<<ngs_blocks(n, 256, 148 * 4), 256, 0, (cudaStream_t)s>>>(a, b, n, out_dev);
+  if (n > 0) { ngs_count_launch(); dot64_kernel<<<ngs_blocks(n, 256, 148 * 4), 256, 0, (cudaStream_t)s>>>(a, b, n, out_dev); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -435,7 +463,7 @@ extern "C" int ngs_dot64(const double* a, const double* b, int64_t n, double* ou
 extern "C" int ngs_axpby64(int64_t n, double alpha, const double* x, double beta, double* y, ngs_stream s) {
   if (n < 0 || (n > 0 && (!x || !y))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  axpby64_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(n, alpha, x, beta, y);
+  { ngs_count_launch(); axpby64_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(n, alpha, x, beta, y); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -443,7 +471,7 @@ extern "C" int ngs_axpby64(int64_t n, double alpha, const double* x, double beta
 extern "C" int ngs_mul64(int64_t n, const double* a, const double* b, double* out, ngs_stream s) {
   if (n < 0 || (n > 0 && (!a || !b || !out))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  mul64_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(n, a, b, out);
+  { ngs_count_launch(); mul64_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(n, a, b, out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

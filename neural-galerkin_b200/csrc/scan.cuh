@@ -108,9 +108,9 @@ int ngs_scan(Load ld, Store st, int64_t n, int64_t* total, void* ws, size_t ws_b
   const int64_t tiles = ngs_scan_tiles(n);
   if (tiles > 0x7fffffffLL) return NGS_ERR_INVALID_ARG;
   int64_t* tile_sums = static_cast<int64_t*>(ws);
-  scan_reduce_kernel<<<(unsigned)tiles, NGS_SCAN_THREADS, 0, s>>>(ld, n, tile_sums);
-  scan_tiles_kernel<<<1, 1024, 0, s>>>(tile_sums, tiles, total);
-  scan_apply_kernel<<<(unsigned)tiles, NGS_SCAN_THREADS, 0, s>>>(ld, st, n, tile_sums);
+  { ngs_count_launch(); scan_reduce_kernel<<<(unsigned)tiles, NGS_SCAN_THREADS, 0, s>>>(ld, n, tile_sums); }
+  { ngs_count_launch(); scan_tiles_kernel<<<1, 1024, 0, s>>>(tile_sums, tiles, total); }
+  { ngs_count_launch(); scan_apply_kernel<<<(unsigned)tiles, NGS_SCAN_THREADS, 0, s>>>(ld, st, n, tile_sums); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

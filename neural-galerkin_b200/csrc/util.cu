@@ -1,4 +1,5 @@
 // Status strings, CUDA error capture, device-wide scans and small reductions.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include "ngs_common.cuh"
@@ -12,6 +13,11 @@ int ngs_set_cuda_error(cudaError_t e) {
 }
 
 extern "C" const char* ngs_last_cuda_error(void) { return g_cuda_error; }
+
+static std::atomic<long long> g_launches{0};
+void ngs_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" int64_t ngs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+extern "C" void ngs_reset_launch_count(void) { g_launches.store(0, std::memory_order_relaxed); }
 
 extern "C" int ngs_version(void) { return 10000; }
 
@@ -106,9 +112,9 @@ extern "C" int ngs_points_bbox(const float* xyz, int64_t n, float* bbox_dev, ngs
   if (n <= 0 || !xyz || !bbox_dev) return NGS_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)s;
   unsigned int* b = reinterpret_cast<unsigned int*>(bbox_dev);
-  bbox_init_kernel<<<1, 32, 0, st>>>(b);
-  bbox_kernel<<<ngs_blocks(n, 256, 148 * 8), 256, 0, st>>>(xyz, n, b);
-  bbox_decode_kernel<<<1, 32, 0, st>>>(b);
+  { ngs_count_launch(); bbox_init_kernel<<<1, 32, 0, st>>>(b); }
+  { ngs_count_launch(); bbox_kernel<<<ngs_blocks(n, 256, 148 * 8), 256, 0, st>>>(xyz, n, b); }
+  { ngs_count_launch(); bbox_decode_kernel<<<1, 32, 0, st>>>(b); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -134,7 +140,7 @@ extern "C" int ngs_weighted_sum(const float* v, const float* w, int64_t n, doubl
   if (n < 0 || !v || !sums_dev) return NGS_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)s;
   cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), st);
-  if (n > 0) weighted_sum_kernel<<<ngs_blocks(n, 256, 148 * 4), 256, 0, st>>>(v, w, n, sums_dev);
+  if (n > 0) { ngs_count_launch(); weighted_sum_kernel<<<ngs_blocks(n, 256, 148 * 4), 256, 0, st>>>(v, w, n, sums_dev); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

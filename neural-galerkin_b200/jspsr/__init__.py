@@ -13,16 +13,16 @@ __version_info__ = (1, 0, 0)
 
 
 def _to_device(a, device):
+    """Input -> float32 CUDA tensor; returns (tensor, kind) with kind "cuda", "cpu" (torch) or "numpy"."""
     import numpy as np
     import torch
     if isinstance(a, torch.Tensor):
-        return a.to(device=device, dtype=torch.float32).contiguous(), True
+        kind = "cuda" if a.is_cuda else "cpu"
+        return a.to(device=device, dtype=torch.float32, non_blocking=True).contiguous(), kind
     if hasattr(a, "numpy") and not isinstance(a, np.ndarray):     # jittor Var and friends
         a = a.numpy()
     host = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32))
-    if torch.cuda.is_available():
-        host = host.pin_memory()
-    return host.to(device, non_blocking=True), False
+    return host.to(device), "numpy"
 
 
 def reconstruct(xyz, normal, voxel_size: float, depth: int = 4, min_density: float = 32.0,
@@ -38,8 +38,9 @@ def reconstruct(xyz, normal, voxel_size: float, depth: int = 4, min_density: flo
     :param screen_alpha: weight of the screening term
     :param solver: per-level linear solver (``"pcg"`` reproduces the reference's FP32 PCG with
         tol 1e-5; the default is FP32 PCG with FP64 dots and FP64 residual replacement)
-    :return: vertices (V, 3) float32, triangles (T, 3) int64 -- torch CUDA tensors when the
-        inputs were torch tensors, numpy arrays otherwise
+    :return: vertices (V, 3) float32, triangles (T, 3) int64 -- torch tensors on the inputs'
+        device when the inputs were torch tensors (CPU inputs are copied in and the mesh copied
+        back), numpy arrays otherwise
     """
     import torch
     from .core.pipeline import Reconstruction
@@ -49,12 +50,12 @@ def reconstruct(xyz, normal, voxel_size: float, depth: int = 4, min_density: flo
     if not torch.cuda.is_available():
         raise RuntimeError("jspsr.reconstruct needs a CUDA device (libngs has no CPU path)")
     dev = torch.device("cuda", torch.cuda.current_device())
-    xyz_d, is_torch = _to_device(xyz, dev)
+    xyz_d, kind = _to_device(xyz, dev)
     nrm_d, _ = _to_device(normal, dev)
     rec = Reconstruction(xyz_d, nrm_d, voxel_size, depth, min_density, screen_alpha, solver=solver)
     v, f = rec.run(n_upsample)
-    if return_reconstruction:
-        return (v, f, rec) if is_torch else (v.cpu().numpy(), f.cpu().numpy(), rec)
-    if is_torch:
-        return v, f
-    return v.cpu().numpy(), f.cpu().numpy()
+    if kind == "cpu":
+        v, f = v.cpu(), f.cpu()
+    elif kind == "numpy":
+        v, f = v.cpu().numpy(), f.cpu().numpy()
+    return (v, f, rec) if return_reconstruction else (v, f)

@@ -48,6 +48,8 @@ _SIGS = {
     "ngs_status_string": ([C.c_int], C.c_char_p),
     "ngs_last_cuda_error": ([], C.c_char_p),
     "ngs_version": ([], C.c_int),
+    "ngs_launch_count": ([], i64),
+    "ngs_reset_launch_count": ([], None),
     "ngs_hash_coords": ([vp, C.c_int, i64, C.c_int, vp, vp], C.c_int),
     "ngs_kernel_hash": ([vp, C.c_int, i64, C.c_int, vp, i64, vp, vp], C.c_int),
     "ngs_hash_table_slots": ([i64, C.c_int], i64),

@@ -41,7 +41,7 @@ class SolverSpec:
     maxiter: int = -1
     res_fix: bool = False
     replace: int = 50
-    timeout: float = 30.0
+    timeout: float = 20.0
 
     @property
     def mode(self):
@@ -157,6 +157,8 @@ class Reconstruction:
         self.levels: list[Level] = []
         self.t = timings
         self.solve_stats = {}
+        self.profile_pcg = False
+        self._pcg_events = {}
 
     def _mark(self, name):
         if self.t is not None:
@@ -289,7 +291,7 @@ class Reconstruction:
         lv.rhs = rhs
         return rhs
 
-    def _solve_level(self, lv: Level):
+    def _solve_level(self, lv: Level, d: int = 0):
         spec = self.solver
         lv.x32 = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
         lv.x64 = torch.empty(lv.n, dtype=torch.float64, device=self.dev)
@@ -309,8 +311,14 @@ class Reconstruction:
         cfg.res_fix, cfg.replace_every, cfg.blocks, cfg.timeout_s = int(spec.res_fix), spec.replace, 0, spec.timeout
         ws_bytes = L.load().ngs_pcg_workspace_bytes(lv.n, spec.mode)
         ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.dev)
+        if self.profile_pcg:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
         L.call("ngs_pcg_solve", L.C.byref(sysd), L.C.byref(cfg), L.ptr(ws), ws_bytes, L.ptr(lv.info),
                L.ptr(lv.resid), L.stream())
+        if self.profile_pcg:
+            ev[1].record()
+            self._pcg_events[d] = ev
         if spec.mode == L.PCG_REFERENCE:
             lv.x64 = lv.x32.double()
         lv._keep = (ws, b32)
@@ -334,7 +342,8 @@ class Reconstruction:
             return float(dot.item())
         atol = spec.tol * math.sqrt(dotv(b, b))
         rho, it = 0.0, 0
-        while spec.maxiter < 0 or it < spec.maxiter:
+        cap = 20000 if spec.maxiter < 0 else min(spec.maxiter, 20000)
+        while it < cap:
             L.call("ngs_mul64", n, L.ptr(dinv), L.ptr(r), L.ptr(z), st)
             rho1, rho = rho, dotv(r, z)
             if it == 0:
@@ -351,14 +360,23 @@ class Reconstruction:
         lv.x64 = x
         lv.x32.copy_(x)
         lv.info[0] = it
+        lv.resid[0] = math.sqrt(dotv(r, r))
+        lv.resid[1] = atol / spec.tol if spec.tol > 0 else 0.0
 
     def solve(self):
         """Coarse-to-fine solve (reconstructor.py:122-189)."""
         for d in range(self.depth - 1, -1, -1):
             self._rhs(d)
-            self._solve_level(self.levels[d])
-        self._mark("solve")
+            self._mark(f"rhs{d}")
+            self._solve_level(self.levels[d], d)
+            self._mark(f"pcg{d}")
         return self
+
+    @property
+    def pcg_ms(self):
+        """Device time of each level's PCG launch (needs profile_pcg = True before solve)."""
+        torch.cuda.synchronize()
+        return {d: e[0].elapsed_time(e[1]) for d, e in self._pcg_events.items()}
 
     def check_solves(self):
         """Read back iteration counts / status of every level (one sync)."""

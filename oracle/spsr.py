@@ -340,7 +340,7 @@ def stiffness(grids, tabs, d, dd):
 
 
 def solve_multigrid(xyz32, nrm32, vs, depth=4, min_density=32.0, screen_alpha=4.0,
-                    screen_delta=0.1, levels=None, keep_lhs=False) -> Solution:
+                    screen_delta=0.1, levels=None, keep_lhs=False, cg_tol=None) -> Solution:
     """Tree build + splat + coarse-to-fine Galerkin solve (``__init__.py:34-54``, ``reconstructor.py:79-195``)."""
     xyz32 = np.ascontiguousarray(xyz32, dtype=F32)
     nrm32 = np.ascontiguousarray(nrm32, dtype=F32)
@@ -384,7 +384,10 @@ def solve_multigrid(xyz32, nrm32, vs, depth=4, min_density=32.0, screen_alpha=4.
         if alpha > 0:
             a = a + sf * alpha * (phis[d].T @ phis[d])
         a = a.tocsc()
-        sol.x[d] = spla.spsolve(a, rhs) if n < 3000 else _cg64(a, rhs)
+        if cg_tol is not None:
+            sol.x[d] = _cg64(a, rhs, tol=cg_tol)        # the CPU baseline: FP64 CSR + Jacobi CG
+        else:
+            sol.x[d] = spla.spsolve(a, rhs) if n < 3000 else _cg64(a, rhs)
         sol.rhs[d] = rhs
         if keep_lhs:
             sol.lhs[d] = a.tocsr()
@@ -606,9 +609,10 @@ def extract_multiscale_mesh(sol: Solution, xyz32, n_upsample=2, max_depth=100) -
                 n_primal={d: epb[d].shape[0] for d in epb}, mean_chi=mc)
 
 
-def reconstruct(xyz, normal, voxel_size, depth=4, min_density=32.0, screen_alpha=4.0):
+def reconstruct(xyz, normal, voxel_size, depth=4, min_density=32.0, screen_alpha=4.0, cg_tol=None):
     """End-to-end oracle of ``jspsr.reconstruct`` (``jspsr/__init__.py:8-61``)."""
     xyz32 = np.asarray(xyz, dtype=F32)
-    sol = solve_multigrid(xyz32, np.asarray(normal, dtype=F32), voxel_size, depth, min_density, screen_alpha)
+    sol = solve_multigrid(xyz32, np.asarray(normal, dtype=F32), voxel_size, depth, min_density, screen_alpha,
+                          cg_tol=cg_tol)
     mesh = extract_multiscale_mesh(sol, xyz32, n_upsample=2)
     return mesh, sol

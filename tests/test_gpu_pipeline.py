@@ -137,7 +137,7 @@ def test_plain_fp64_comparator(cases):
     g, sol, _ = cases["torus_small"]
     rec, _, _ = run_gpu(g, solver="plain-fp64@tol=1e-10")
     for d, lv in enumerate(rec.levels):
-        assert rel(lv.x64.cpu().numpy(), sol.x[d]) < 1e-7
+        assert rel(lv.x64.cpu().numpy(), sol.x[d]) < 1e-6                  # system assembled from FP32 basis values
 
 
 def test_public_reconstruct_roundtrip(cases):
