@@ -25,11 +25,18 @@
 #include <cmath>
 #include "ngs_common.cuh"
 
-constexpr int PCG_THREADS = 256;
-constexpr int PCG_ROW_LANES = 16;   // lanes per row in the SpMV
+constexpr int PCG_THREADS = 512;
+constexpr int PCG_ROW_LANES = 4;       // lanes per row in the per-row reduction
+constexpr int PCG_TILE_NNZ = 5120;     // non-zeros per shared-memory tile (stage)
+constexpr int PCG_ROW_COST = 8;        // planning cost of a row on top of its non-zeros
+constexpr int PCG_TILE_BODY = PCG_TILE_NNZ - 264;   // cost budget of a tile; whole rows extend it by < 264
+constexpr int PCG_TILE_ROWS = (PCG_TILE_BODY + 264) / (PCG_ROW_COST + 1) + 1;   // rows a tile can hold
+constexpr int PCG_MAX_TILES = 2048;    // tiles a block can own
+constexpr int PCG_STAGES = 2;
 
 struct PcgArgs {
   int64_t n;
+  int64_t nnz;
   const int64_t* rowptr;
   const int32_t* cols;
   const void* vals;          // recurrence matrix (float or double)
@@ -53,7 +60,7 @@ struct PcgArgs {
   double tol;
   int max_iter;
   int replace_every;         // <= 0: never
-  double inner_rtol;          // MIXED: relative reduction of an inner solve
+  double inner_rtol;         // MIXED: relative reduction of an inner solve
   unsigned long long wait_ns;     // bound of one barrier wait
   unsigned long long* deadline;   // absolute global-timer deadline, set at the first reduction
   unsigned long long budget_ns;   // time budget of the whole solve
@@ -70,6 +77,189 @@ NGS_DEV unsigned long long global_ns() {
 
 template <typename T>
 NGS_DEV T ld_cg(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
+
+// ----------------------------------------------------------------------------- bulk copies (no multicast)
+NGS_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+NGS_DEV void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+NGS_DEV void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+NGS_DEV void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+NGS_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+NGS_DEV bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+
+// Per-block state of the tiled SpMV: rows [row0, row1) owned by the block, split into tiles of
+// whole rows of at most PCG_TILE_NNZ non-zeros; tile t covers rows [tiles[t], tiles[t+1]).
+struct BlockRows {
+  int64_t row0, row1, ebase;
+  int ntiles;
+  int32_t* tiles;              // shared: first row of tile t (block-relative), [ntiles + 1]
+  int32_t* tile_e;             // shared: first non-zero of tile t (relative to ebase), [ntiles + 1]
+  int32_t* srp;                // shared: row offsets of the current tile, [PCG_TILE_ROWS + 1]
+  double2* aux;                // shared: epilogue operands of the current tile's rows, [PCG_TILE_ROWS]
+  double* prod;                // shared: products of the current tile, [PCG_TILE_NNZ]
+  unsigned long long* bars;    // shared, one mbarrier per stage
+  char* stage;                 // shared, PCG_STAGES stages
+  size_t stage_bytes;
+  unsigned phase;              // parity bits, one per stage (block-uniform)
+};
+
+// Block b owns the rows whose first non-zero lies in [b * nnz / B, (b + 1) * nnz / B).
+NGS_DEV int64_t first_row_at(const int64_t* __restrict__ rp, int64_t n, int64_t e) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (rp[mid] < e) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Tile starts: a row costs its non-zeros plus PCG_ROW_COST; tile k holds the rows whose last cost unit
+// falls in [k, k+1) * PCG_TILE_BODY (block-relative), so a tile holds at most PCG_TILE_NNZ non-zeros and
+// PCG_TILE_ROWS rows.  Rows longer than PCG_MAX_ROW, or empty, are rejected.  Returns false for such a block.
+constexpr int PCG_MAX_ROW = 250;
+
+NGS_DEV bool plan_tiles(const PcgArgs& a, BlockRows& br) {
+  __shared__ int64_t bounds[2];
+  __shared__ int nt, bad;
+  if (threadIdx.x == 0) {
+    const int64_t B = a.nblocks;
+    bounds[0] = first_row_at(a.rowptr, a.n, (a.nnz * (int64_t)blockIdx.x) / B);
+    bounds[1] = blockIdx.x + 1 == a.nblocks ? a.n : first_row_at(a.rowptr, a.n, (a.nnz * ((int64_t)blockIdx.x + 1)) / B);
+    nt = 0;
+    bad = 0;
+  }
+  __syncthreads();
+  br.row0 = bounds[0];
+  br.row1 = bounds[1];
+  const int64_t base = br.row0 < br.row1 ? a.rowptr[br.row0] : 0;
+  for (int64_t r = br.row0 + threadIdx.x; r < br.row1; r += blockDim.x) {
+    const int64_t e0 = a.rowptr[r], e1 = a.rowptr[r + 1];
+    if (e1 - e0 > PCG_MAX_ROW || e1 <= e0) bad = 1;   // SPD rows hold at least their diagonal
+    // index of the tile holding the row's last cost unit
+    const int64_t d1 = (e1 - base) + (int64_t)PCG_ROW_COST * (r + 1 - br.row0);
+    const int64_t d0 = (e0 - base) + (int64_t)PCG_ROW_COST * (r - br.row0);
+    const int64_t k = (d1 + PCG_TILE_BODY - 1) / PCG_TILE_BODY - 1;
+    const int64_t kp = r == br.row0 ? -1 : (d0 + PCG_TILE_BODY - 1) / PCG_TILE_BODY - 1;
+    for (int64_t t = kp + 1; t <= k && t < PCG_MAX_TILES; t++) br.tiles[t] = (int32_t)(r - br.row0);
+    if (r + 1 == br.row1) nt = (int)(k + 1 < PCG_MAX_TILES ? k + 1 : PCG_MAX_TILES);
+  }
+  __syncthreads();
+  br.ntiles = br.row0 < br.row1 ? (nt > 0 ? nt : 1) : 0;
+  br.ebase = base;
+  if (threadIdx.x == 0 && br.ntiles > 0) {
+    br.tiles[0] = 0;
+    br.tiles[br.ntiles] = (int32_t)(br.row1 - br.row0);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t <= br.ntiles; t += blockDim.x) br.tile_e[t] = (int32_t)(a.rowptr[br.row0 + br.tiles[t]] - base);
+  __syncthreads();
+  return bad == 0;
+}
+
+// Issue the bulk copies of tile t into stage st: the 16-byte aligned body of its column and value
+// ranges; the ragged tail (< 4 elements) is read from global memory by the consumer.
+template <typename MT>
+NGS_DEV void issue_tile(const PcgArgs& a, const MT* vals, BlockRows& br, int t, int st) {
+  if (threadIdx.x != 0) return;
+  const int64_t e0 = br.ebase + br.tile_e[t], e1 = br.ebase + br.tile_e[t + 1];
+  constexpr int64_t VA = 16 / sizeof(MT);
+  const int64_t c0 = e0 & ~3ll, c1 = e1 & ~3ll, v0 = e0 & ~(VA - 1), v1 = e1 & ~(VA - 1);
+  const unsigned cb = (unsigned)((c1 > c0 ? c1 - c0 : 0) * 4), vb = (unsigned)((v1 > v0 ? v1 - v0 : 0) * sizeof(MT));
+  char* dst = br.stage + st * br.stage_bytes;
+  mbar_expect_tx(&br.bars[st], cb + vb);
+  if (cb) bulk_g2s(dst, a.cols + c0, cb, &br.bars[st]);
+  if (vb) bulk_g2s(dst + PCG_TILE_NNZ * 4, vals + v0, vb, &br.bars[st]);
+}
+
+// y = A v over the block's rows; epi(row, acc) consumes each row's product and returns a
+// contribution to the block's partial sum.  Returns false if a copy wait timed out.
+template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
+NGS_DEV bool spmv_tiles(const PcgArgs& a, const MT* __restrict__ vals, const VT* __restrict__ v, BlockRows& br,
+                        Pre pre, Epi epi, double& dsum) {
+  const int lane = threadIdx.x & (PCG_ROW_LANES - 1);
+  const int group = threadIdx.x / PCG_ROW_LANES, ngroups = PCG_THREADS / PCG_ROW_LANES;
+  const unsigned gmask = ((1u << PCG_ROW_LANES) - 1u) << ((threadIdx.x & 31) & ~(PCG_ROW_LANES - 1));
+  constexpr int64_t VA = 16 / sizeof(MT);
+  for (int t = 0; t < PCG_STAGES && t < br.ntiles; t++) issue_tile(a, vals, br, t, t);
+  bool ok = true;
+  for (int t = 0; t < br.ntiles; t++) {
+    const int st = t % PCG_STAGES;
+    const unsigned par = (br.phase >> st) & 1u;
+    int mine = 1;
+    if (ok) {
+      const unsigned long long t0 = global_ns();
+      while (!mbar_try_wait(&br.bars[st], par)) {
+        if (global_ns() - t0 > a.wait_ns) {
+          atomicExch(a.error, NGS_ERR_TIMEOUT);
+          mine = 0;
+          break;
+        }
+      }
+    }
+    ok = __syncthreads_and(ok && mine) != 0;   // block-uniform outcome of the wait
+    br.phase ^= 1u << st;
+    if (!ok) continue;             // a copy wait gave up: issue nothing more, consume nothing
+    const char* sm = br.stage + st * br.stage_bytes;
+    const int32_t* scol = reinterpret_cast<const int32_t*>(sm);
+    const MT* sval = reinterpret_cast<const MT*>(sm + PCG_TILE_NNZ * 4);
+    const int64_t r_lo = br.row0 + br.tiles[t], r_hi = br.row0 + br.tiles[t + 1];
+    const int64_t e0 = br.ebase + br.tile_e[t], e1 = br.ebase + br.tile_e[t + 1];
+    const int64_t c0 = e0 & ~3ll, c1 = e1 & ~3ll, v0 = e0 & ~(VA - 1), v1 = e1 & ~(VA - 1);
+    ACC* prod = reinterpret_cast<ACC*>(br.prod);
+    // pass 1: every product of the tile.  Fully unrolled and predicated, so that each thread has
+    // all of its gathers in flight at once; the tile's row offsets are staged alongside.
+    constexpr int PER = (PCG_TILE_NNZ + PCG_THREADS - 1) / PCG_THREADS;
+    int32_t cc[PER];
+    MT mm[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int64_t j = e0 + threadIdx.x + (int64_t)k * PCG_THREADS;
+      cc[k] = -1;
+      mm[k] = (MT)0;
+      if (j < e1) {
+        cc[k] = j < c1 ? scol[j - c0] : __ldg(a.cols + j);
+        mm[k] = j < v1 ? sval[j - v0] : __ldg(vals + j);
+      }
+    }
+    VT vv[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) vv[k] = cc[k] >= 0 ? v[cc[k]] : (VT)0;
+    for (int64_t rr = r_lo + threadIdx.x; rr <= r_hi; rr += PCG_THREADS) {
+      br.srp[rr - r_lo] = (int32_t)(a.rowptr[rr] - e0);
+      if (rr < r_hi) br.aux[rr - r_lo] = pre(rr);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int64_t j = e0 + threadIdx.x + (int64_t)k * PCG_THREADS;
+      if (j < e1) prod[j - e0] = (ACC)mm[k] * (ACC)vv[k];
+    }
+    __syncthreads();
+    // pass 2: per-row sums from shared memory
+    for (int64_t row = r_lo + group; row < r_hi; row += ngroups) {
+      const int beg = br.srp[row - r_lo], end = br.srp[row - r_lo + 1];
+      ACC acc = (ACC)0;
+      for (int k = beg + lane; k < end; k += PCG_ROW_LANES) acc += prod[k];
+#pragma unroll
+      for (int o = PCG_ROW_LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
+      if (lane == 0) dsum += epi(row, (double)acc, br.aux[row - r_lo]);
+    }
+    __syncthreads();
+    if (t + PCG_STAGES < br.ntiles) issue_tile(a, vals, br, t + PCG_STAGES, st);
+  }
+  return ok;
+}
 
 // Block sums of NV doubles -> per-block partials -> fixed-order grid reduction.
 template <int NV>
@@ -141,57 +331,33 @@ NGS_DEV bool reduce_barrier(const PcgArgs& a, const double (&v)[NV], double (&ou
   return ok != 0;
 }
 
-NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0; }
-
 NGS_DEV bool plain_barrier(const PcgArgs& a) {
   double v[1] = {0.0}, o[1];
   return reduce_barrier<1>(a, v, o);
 }
 
-// Row-parallel SpMV, PCG_ROW_LANES lanes per row; the group leader hands the row's
-// product to `epi(row, acc)`, which writes whatever the row owns and returns a
-// contribution to the block's partial sum.  Outputs of an SpMV are only ever
-// consumed by its own epilogue or after a grid barrier.
-template <typename MT, typename VT, typename ACC, typename Epi>
-NGS_DEV double spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* __restrict__ v, Epi epi) {
-  const int sub = threadIdx.x & (PCG_ROW_LANES - 1);
-  const unsigned gmask = ((1u << PCG_ROW_LANES) - 1u) << ((threadIdx.x & 31) & ~(PCG_ROW_LANES - 1));
-  const int64_t groups = (int64_t)gridDim.x * (PCG_THREADS / PCG_ROW_LANES);
-  double dsum = 0.0;
-  for (int64_t row = ((int64_t)blockIdx.x * PCG_THREADS + threadIdx.x) / PCG_ROW_LANES;; row += groups) {
-    if (!__any_sync(0xffffffffu, row < a.n)) break;
-    if (row < a.n) {
-      const int64_t beg = a.rowptr[row], end = a.rowptr[row + 1];
-      ACC acc = (ACC)0;
-      for (int64_t j = beg + sub; j < end; j += PCG_ROW_LANES)
-        acc += (ACC)__ldg(vals + j) * (ACC)v[__ldg(a.cols + j)];
-#pragma unroll
-      for (int o = PCG_ROW_LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
-      if (sub == 0) dsum += epi(row, (double)acc);
-    }
-  }
-  return dsum;
-}
+NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0; }
 
 template <int MODE>
 struct PcgTypes;
-template <> struct PcgTypes<NGS_PCG_REFERENCE> { using MT = float; using VT = float; using RT = float; };
-template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = double; using RT = double; };
-template <> struct PcgTypes<NGS_PCG_FP64> { using MT = double; using VT = double; using RT = double; };
+template <> struct PcgTypes<NGS_PCG_REFERENCE> { using MT = float; using VT = float; using RT = float; using ACC = float; };
+template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = double; using RT = double; using ACC = double; };
+template <> struct PcgTypes<NGS_PCG_FP64> { using MT = double; using VT = double; using RT = double; using ACC = double; };
 
-// Recurrence SpMV of a mode: REFERENCE is all FP32 (as cuSPARSE SpMV in the reference);
-// MIXED reads FP32 matrix values and accumulates in FP64; FP64 is all FP64.
-template <int MODE, typename VT, typename Epi>
-NGS_DEV double spmv_mode(const PcgArgs& a, const VT* v, Epi epi) {
-  if constexpr (MODE == NGS_PCG_FP64) return spmv_rows<double, VT, double>(a, static_cast<const double*>(a.vals), v, epi);
-  else if constexpr (MODE == NGS_PCG_MIXED) return spmv_rows<float, VT, double>(a, static_cast<const float*>(a.vals), v, epi);
-  else return spmv_rows<float, VT, float>(a, static_cast<const float*>(a.vals), v, epi);
+// Bytes of dynamic shared memory the kernel of a mode needs (tile stages + tile plan + mbarriers).
+constexpr size_t pcg_stage_bytes(int mode) { return (size_t)PCG_TILE_NNZ * (4 + (mode == NGS_PCG_REFERENCE ? 4 : 8)); }
+constexpr size_t pcg_smem_bytes(int mode) {
+  return (size_t)PCG_STAGES * pcg_stage_bytes(mode) + (size_t)PCG_TILE_NNZ * 8 + (size_t)PCG_TILE_ROWS * 16 +
+         ((PCG_TILE_ROWS + 4) * 4 + 15) / 16 * 16 + 2 * (PCG_MAX_TILES + 4) * 4 + 64;
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
+__global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
+  using MT = typename PcgTypes<MODE>::MT;
   using VT = typename PcgTypes<MODE>::VT;
   using RT = typename PcgTypes<MODE>::RT;
+  using ACC = typename PcgTypes<MODE>::ACC;
+  extern __shared__ __align__(128) char smem[];
   const RT* b = static_cast<const RT*>(a.b);
   RT* x = static_cast<RT*>(a.x);
   RT* r = static_cast<RT*>(a.r);
@@ -199,26 +365,60 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
   VT* s = static_cast<VT*>(a.s);
   VT* u = static_cast<VT*>(a.u);
   VT* w = static_cast<VT*>(a.w);
-  const int64_t n = a.n;
-  const int64_t t0 = ngs_gtid(), ts = ngs_gstride();
-  const int sqrt_n = (int)ceil(sqrt((double)n));
+  const MT* vals = static_cast<const MT*>(a.vals);
+  const int sqrt_n = (int)ceil(sqrt((double)a.n));
 
-  // w = A u; returns (w, u)
-  auto w_epi = [&](int64_t row, double acc) -> double {
+  // shared layout: [stages][cols | vals] , tile plan, mbarriers
+  constexpr size_t stage_bytes = pcg_stage_bytes(MODE);
+  BlockRows br;
+  char* sp = smem;
+  br.stage = sp;
+  br.stage_bytes = stage_bytes;
+  sp += PCG_STAGES * stage_bytes;
+  br.prod = reinterpret_cast<double*>(sp);
+  sp += (size_t)PCG_TILE_NNZ * 8;
+  br.aux = reinterpret_cast<double2*>(sp);
+  sp += (size_t)PCG_TILE_ROWS * 16;
+  br.srp = reinterpret_cast<int32_t*>(sp);
+  sp += ((size_t)(PCG_TILE_ROWS + 4) * 4 + 15) / 16 * 16;
+  br.tiles = reinterpret_cast<int32_t*>(sp);
+  sp += (size_t)(PCG_MAX_TILES + 4) * 4;
+  br.tile_e = reinterpret_cast<int32_t*>(sp);
+  sp += (size_t)(PCG_MAX_TILES + 4) * 4;
+  br.bars = reinterpret_cast<unsigned long long*>(sp);
+  br.phase = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < PCG_STAGES; i++) mbar_init(&br.bars[i], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const bool rows_ok = plan_tiles(a, br);
+  const int64_t i0 = br.row0 + threadIdx.x, i1 = br.row1, is = PCG_THREADS;
+
+  // w = A u; returns (w, u).  The row's u is prefetched during the tile's product pass.
+  auto w_pre = [&](int64_t row) -> double2 { return make_double2((double)u[row], 0.0); };
+  auto w_epi = [&](int64_t row, double acc, double2 ax) -> double {
     w[row] = (VT)acc;
-    return acc * (double)u[row];
+    return acc * ax.x;
   };
-  // r = b - A x, u = M r; returns (r, r)
-  auto true_res_epi = [&](int64_t row, double acc) -> double {
-    const RT ri = (RT)((double)b[row] - acc);
+  // r = b - A x, u = M r; returns (r, r).  b and 1/diag of the row are prefetched.
+  auto res_pre = [&](int64_t row) -> double2 { return make_double2((double)b[row], (double)a.inv_diag[row]); };
+  auto true_res_epi = [&](int64_t row, double acc, double2 ax) -> double {
+    const RT ri = (RT)(ax.x - acc);
     r[row] = ri;
-    u[row] = (VT)((double)a.inv_diag[row] * (double)ri);
+    u[row] = (VT)(ax.y * (double)ri);
     return (double)ri * (double)ri;
   };
+  // The FP64 true-residual SpMV of MIXED mode streams the FP64 values through the same stages
+  // (the stage holds PCG_TILE_NNZ doubles in MIXED mode); REFERENCE mode replaces with the FP32 matrix.
+  auto spmv_true = [&](double& sum) -> bool {
+    if constexpr (MODE == NGS_PCG_MIXED) return spmv_tiles<double, RT, double>(a, a.vals64, x, br, res_pre, true_res_epi, sum);
+    else return spmv_tiles<MT, RT, ACC>(a, vals, x, br, res_pre, true_res_epi, sum);
+  };
 
-  // init: x = 0, r = b, u = M r, p = s = 0; partial (b, b)
-  double part[3] = {0.0, 0.0, 0.0}, res[3];
-  for (int64_t i = t0; i < n; i += ts) {
+  // init: x = 0, r = b, u = M r, p = s = 0; partial (b, b); part[1] flags rows too long for a tile
+  double part[3] = {0.0, rows_ok ? 0.0 : 1.0, 0.0}, res[3];
+  for (int64_t i = i0; i < i1; i += is) {
     const RT bi = b[i];
     x[i] = (RT)0;
     r[i] = bi;
@@ -228,11 +428,18 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
     part[0] += (double)bi * (double)bi;
   }
   if (!reduce_barrier<3>(a, part, res)) return;
+  if (res[1] > 0.0) {                                    // every block sees the same flag: no copy was issued
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.info[0] = 0;
+      a.info[1] = NGS_ERR_INVALID_ARG;
+    }
+    return;
+  }
   const double bnorm = sqrt(res[0]);
   const double atol = a.tol * bnorm;
   part[0] = part[1] = part[2] = 0.0;
-  part[1] = spmv_mode<MODE>(a, u, w_epi);
-  for (int64_t i = t0; i < n; i += ts) {
+  if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
+  for (int64_t i = i0; i < i1; i += is) {
     part[0] += (double)r[i] * (double)u[i];
     part[2] += (double)r[i] * (double)r[i];
   }
@@ -249,8 +456,10 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
     const bool replace =
         (MODE == NGS_PCG_MIXED && a.replace_every > 0 && (it + 1) % a.replace_every == 0) ||
         (MODE == NGS_PCG_REFERENCE && a.replace_every > 0 && (it + 1) % sqrt_n == 0);
-    // phase A (own rows)
-    for (int64_t i = t0; i < n; i += ts) {
+    // phase A (own rows); the dots (r,u), (r,r) of the new residual are taken here
+    part[0] = part[1] = part[2] = 0.0;
+#pragma unroll 4
+    for (int64_t i = i0; i < i1; i += is) {
       const VT pi = (VT)((double)u[i] + beta * (double)p[i]);
       const VT si = (VT)((double)w[i] + beta * (double)s[i]);
       p[i] = pi;
@@ -258,25 +467,25 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
       x[i] = (RT)((double)x[i] + alpha * (double)pi);
       if (!replace) {
         const RT ri = (RT)((double)r[i] - alpha * (double)si);
+        const VT ui = (VT)((double)a.inv_diag[i] * (double)ri);
         r[i] = ri;
-        u[i] = (VT)((double)a.inv_diag[i] * (double)ri);
+        u[i] = ui;
+        part[0] += (double)ri * (double)ui;
+        part[2] += (double)ri * (double)ri;
       }
     }
     if (replace) {
       // residual replacement: r = b - A x (FP64 matrix in MIXED mode, the FP32 one in REFERENCE mode)
       if (!plain_barrier(a)) return;
-      if constexpr (MODE == NGS_PCG_MIXED) spmv_rows<double, RT, double>(a, a.vals64, x, true_res_epi);
-      else spmv_rows<float, RT, float>(a, static_cast<const float*>(a.vals), x, true_res_epi);
+      double rr = 0.0;
+      if (!spmv_true(rr)) return;
+      part[2] = rr;
+      for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       replacements++;
     }
     if (!plain_barrier(a)) return;
-    // phase B
-    part[0] = part[1] = part[2] = 0.0;
-    part[1] = spmv_mode<MODE>(a, u, w_epi);
-    for (int64_t i = t0; i < n; i += ts) {
-      part[0] += (double)r[i] * (double)u[i];
-      part[2] += (double)r[i] * (double)r[i];
-    }
+    // phase B: w = A u and (w, u)
+    if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
     if (!reduce_barrier<3>(a, part, res)) return;
     it++;
     const double gamma_new = res[0];
@@ -287,11 +496,11 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
       // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
       if (!plain_barrier(a)) return;
       part[0] = part[1] = part[2] = 0.0;
-      part[2] = spmv_rows<double, RT, double>(a, a.vals64, x, true_res_epi);
+      if (!spmv_true(part[2])) return;
       replacements++;
+      for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       if (!plain_barrier(a)) return;
-      part[1] = spmv_mode<MODE>(a, u, w_epi);
-      for (int64_t i = t0; i < n; i += ts) part[0] += (double)r[i] * (double)u[i];
+      if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
       if (!reduce_barrier<3>(a, part, res)) return;
       rho = res[2];
       if (sqrt(rho) <= atol) { converged = true; break; }
@@ -308,7 +517,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_kernel(PcgArgs a) {
     gamma = gamma_new;
   }
   if (a.x32_out)
-    for (int64_t i = t0; i < n; i += ts) a.x32_out[i] = (float)x[i];
+    for (int64_t i = i0; i < i1; i += is) a.x32_out[i] = (float)x[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.info[0] = it;
     a.info[1] = converged ? NGS_OK : (timed_out ? NGS_ERR_TIMEOUT : NGS_ERR_NOT_CONVERGED);
@@ -334,18 +543,25 @@ static int launch_pcg(PcgArgs& a, int blocks_req, cudaStream_t st) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, 0);
+  const size_t smem = pcg_smem_bytes(MODE);
+  cudaError_t e = cudaFuncSetAttribute(pcg_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, smem);
   if (per_sm < 1) return NGS_ERR_CUDA;
   int64_t blocks = (int64_t)sms * per_sm;
-  const int64_t need = (a.n * PCG_ROW_LANES + PCG_THREADS - 1) / PCG_THREADS;
+  // small systems: fewer blocks, each with at least a few tiles of work
+  const int64_t need = (a.nnz + (int64_t)PCG_ROW_COST * a.n + 4 * PCG_TILE_BODY - 1) / (4 * PCG_TILE_BODY);
   if (blocks > need) blocks = need > 0 ? need : 1;
+  // a block owns at most PCG_MAX_TILES tiles
+  if ((a.nnz + (int64_t)PCG_ROW_COST * a.n) / blocks + 512 > (int64_t)(PCG_MAX_TILES - 2) * PCG_TILE_BODY)
+    return NGS_ERR_INVALID_ARG;
   if (blocks_req > 0 && blocks_req < blocks) blocks = blocks_req;
   if (blocks > 148 * 32) blocks = 148 * 32;
   a.nblocks = (unsigned int)blocks;
   void* args[] = {&a};
   ngs_count_launch();
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)pcg_kernel<MODE>, dim3((unsigned)blocks), dim3(PCG_THREADS),
-                                              args, 0, st);
+  e = cudaLaunchCooperativeKernel((const void*)pcg_kernel<MODE>, dim3((unsigned)blocks), dim3(PCG_THREADS), args,
+                                  smem, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }
@@ -373,6 +589,7 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   char* base = static_cast<char*>(ws);
   PcgArgs a{};
   a.n = n;
+  a.nnz = sys->nnz;
   a.rowptr = sys->rowptr;
   a.cols = sys->cols;
   a.vals = mode == NGS_PCG_FP64 ? (const void*)sys->vals64 : (const void*)sys->vals32;
