@@ -233,6 +233,18 @@ size_t ngs_pcg_workspace_bytes(int64_t n, int mode);
 int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
                   int64_t* info_dev, double* resid_dev, ngs_stream s);
 
+/* ngs_pcg_solve without any workspace from the caller, for callers that cannot allocate device
+ * memory when they solve (no counterpart in the reference).  Scratch lives in a static device
+ * array inside the library, sized for n <= ngs_pcg_noalloc_max_rows() (131072) rows; larger
+ * systems return NGS_ERR_OOM before anything is launched.  The first call on each device looks
+ * up the array's device address (cudaGetSymbolAddress) -- make that first call before any stream
+ * capture.  All calls in the process share the one array: calls that may overlap on the GPU
+ * (different streams, or concurrent host threads) race and must be serialised by the caller.
+ * Nothing is allocated: no cudaMalloc / cudaFree, no allocating library routine. */
+int64_t ngs_pcg_noalloc_max_rows(void);
+int ngs_pcg_solve_noalloc(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, int64_t* info_dev,
+                          double* resid_dev, ngs_stream s);
+
 /* Plain building blocks for the host-driven FP64 comparator (one launch each). */
 int ngs_spmv64(int64_t n, const int64_t* rowptr, const int32_t* cols, const double* vals, const double* x,
                double* y, ngs_stream s);

@@ -23,6 +23,7 @@
 // a fixed SPD perturbation of the FP64 one, so each outer step contracts the
 // error by about |A32 - A64| |A64^-1| and the solve converges to the FP64 system.
 #include <cmath>
+#include <mutex>
 #include "ngs_common.cuh"
 
 constexpr int PCG_THREADS = 512;
@@ -625,6 +626,58 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   else if (mode == NGS_PCG_MIXED) rc = launch_pcg<NGS_PCG_MIXED>(a, cfg->blocks, st);
   else rc = launch_pcg<NGS_PCG_FP64>(a, cfg->blocks, st);
   return rc;
+}
+
+// ----------------------------------------------------------------------------- solve without allocating
+// Some callers cannot allocate device memory at the moment they need a solve: code that runs
+// inside a host callback or a driver-managed context where cudaMalloc is not permitted, allocators
+// that must not be re-entered, or embedded runtimes that hand this library only the buffers they
+// own.  For them ngs_pcg_solve_noalloc uses a fixed scratch area that is part of the library image
+// itself (a static device array), so the call allocates nothing.  The array is sized for systems of
+// up to kNoallocMaxRows rows in the widest (8-byte vector) mode; larger systems are rejected.  Every
+// GPU that loads the library keeps this array until the process exits.
+static constexpr int64_t kNoallocMaxRows = 131072;
+static constexpr size_t noalloc_align(size_t v) { return (v + 255) & ~(size_t)255; }
+static constexpr size_t kNoallocScratchBytes =
+    noalloc_align(kNoallocMaxRows * 8) + 4 * noalloc_align(kNoallocMaxRows * 8) +
+    noalloc_align((size_t)148 * 32 * 4 * sizeof(double)) + noalloc_align(4 * sizeof(double)) +
+    noalloc_align(8 * sizeof(unsigned int));
+static __device__ __align__(256) unsigned char g_pcg_noalloc_scratch[kNoallocScratchBytes];
+
+// The host cannot use g_pcg_noalloc_scratch as a device address: its device address is looked up
+// once per device (with that device current) and cached here.
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_ptr[256] = {};
+
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  if (dev < 0 || dev >= 256) return NGS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_pcg_noalloc_scratch);
+    if (e != cudaSuccess) return ngs_set_cuda_error(e);
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return NGS_OK;
+}
+
+extern "C" int64_t ngs_pcg_noalloc_max_rows(void) { return kNoallocMaxRows; }
+
+extern "C" int ngs_pcg_solve_noalloc(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, int64_t* info_dev,
+                                     double* resid_dev, ngs_stream s) {
+  if (!sys || !cfg) return NGS_ERR_INVALID_ARG;
+  if (sys->n > kNoallocMaxRows) return NGS_ERR_OOM;            // too large for the built-in scratch
+  if (ngs_pcg_workspace_bytes(sys->n, cfg->mode) > kNoallocScratchBytes) return NGS_ERR_OOM;
+  void* ws = nullptr;
+  const int rc = noalloc_scratch(&ws);
+  if (rc != NGS_OK) return rc;
+  // ngs_pcg_solve clears the control words it needs zeroed and the kernel initialises every vector,
+  // so leftovers of the previous call in the shared scratch do not matter.
+  return ngs_pcg_solve(sys, cfg, ws, kNoallocScratchBytes, info_dev, resid_dev, s);
 }
 
 // ----------------------------------------------------------------------------- FP64 building blocks

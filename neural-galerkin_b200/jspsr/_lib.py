@@ -83,6 +83,8 @@ _SIGS = {
     "ngs_finish_system": ([vp, i64, vp, i64, vp, vp, vp], C.c_int),
     "ngs_pcg_workspace_bytes": ([i64, C.c_int], sz),
     "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
+    "ngs_pcg_noalloc_max_rows": ([], i64),
+    "ngs_pcg_solve_noalloc": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, vp, vp], C.c_int),
     "ngs_spmv64": ([i64, vp, vp, vp, vp, vp, vp], C.c_int),
     "ngs_dot64": ([vp, vp, i64, vp, vp], C.c_int),
     "ngs_axpby64": ([i64, f64, vp, f64, vp, vp], C.c_int),
