@@ -143,3 +143,59 @@ def reference_pickle_tables(n_mult: int = 5):
     return ([p[1] for p in pa], [p[0] for p in pa], [p[1] for p in inv], [p[0] for p in inv],
             [s[0] for s in sh], [s[1] for s in sh], [np.zeros_like(s[0]) for s in sh],
             [np.zeros_like(p[0]) for p in inv])
+
+
+# ----------------------------------------------------------------------------- general 1-D components
+_GL_X, _GL_W = np.polynomial.legendre.leggauss(40)
+
+
+def _gl(fn, lo, hi, breaks):
+    """Gauss-Legendre (40 nodes) on each smooth piece of [lo, hi] between breakpoints."""
+    if hi <= lo:
+        return 0.0
+    pts = sorted({lo, hi, *[b for b in breaks if lo < b < hi]})
+    tot = 0.0
+    for a, b in zip(pts[:-1], pts[1:]):
+        m, h = 0.5 * (a + b), 0.5 * (b - a)
+        tot += h * float(np.dot(_GL_W, fn(m + h * _GL_X)))
+    return tot
+
+
+def component_pair_tables(ci, cj, n_mult: int):
+    """theta / theta-dot tables of two additive components (the integrals of
+    ``jspsr/bases/additive.py:17-28``): lists over m < n_mult of arrays of length 3*2^m + 2."""
+    ff, dfdf = [], []
+    for m in range(n_mult):
+        M = 2 ** m
+        rf, rd = [], []
+        for i in range(3 * M + 2):
+            dx = -1.5 * M - 0.5 + i
+            br = [b - dx for b in ci.breaks] + [b * M for b in cj.breaks]
+            lo, hi = max(-1.5 - dx, -1.5 * M), min(1.5 - dx, 1.5 * M)
+            rf.append(_gl(lambda y: ci.f(y + dx) * cj.f(y / M), lo, hi, br))
+            rd.append(_gl(lambda y: ci.df(y + dx) * cj.df(y / M) / M, lo, hi, br))
+        ff.append(np.asarray(rf))
+        dfdf.append(np.asarray(rd))
+    return ff, dfdf
+
+
+def component_tables(c, n_mult: int):
+    """rho / rho-dot tables of one component (``jspsr/bases/additive.py:31-52``):
+    forward f, df (m < n_mult, length 3*2^m) and inverse f_inv, df_inv (1 <= m < n_mult, length 2^m + 2)."""
+    f, df, fi, dfi = [], [], [], []
+    for m in range(n_mult):
+        M = 2 ** m
+        br = [b * M for b in c.breaks]
+        f.append(np.asarray([_gl(lambda x: c.f(x / M), 1.5 * M - 1 - i, 1.5 * M - i, br) for i in range(3 * M)]))
+        df.append(np.asarray([_gl(lambda x: c.df(x / M) / M, 1.5 * M - 1 - i, 1.5 * M - i, br) for i in range(3 * M)]))
+    for m in range(1, n_mult):
+        M = 2 ** m
+        rows_f, rows_d = [], []
+        for i in range(M + 2):
+            ra = 0.5 - i
+            lb, ub = max(ra, -1.5), min(ra + M, 1.5)
+            rows_f.append(_gl(c.f, lb, ub, c.breaks))
+            rows_d.append(_gl(c.df, lb, ub, c.breaks))
+        fi.append(np.asarray(rows_f))
+        dfi.append(np.asarray(rows_d))
+    return f, df, fi, dfi

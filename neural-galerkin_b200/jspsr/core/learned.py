@@ -1,0 +1,88 @@
+"""The learned-basis (Neural Galerkin) forward/backward on one shape.
+
+The flow of the reference's training step (``models/full_net.py:118-133`` with the splatting of
+``jspsr/__init__.py:36-47``): density-adaptive tree, normals splatted with 1/density weights,
+``Reconstructor.solve_multigrid`` with an ``AdditiveHermite`` basis and per-voxel features, field
+evaluated at query points, MSE loss against a target field, gradients w.r.t. the normals and the
+per-voxel basis features through the autograd graph of assembly, screening and the linear solves.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict
+
+import numpy as np
+import torch
+
+from ..bases.hermite_ns import AdditiveHermite
+from ..bases.additive_components import SinPeaks
+from .hashtree import HashTree
+from .reconstructor import Reconstructor
+
+
+def hermite_basis() -> AdditiveHermite:
+    """AdditiveHermite(n_degrees=6, SinPeaks(1..3)) as configured in ``configs/shapenet/full_net_base.yaml:54-59``."""
+    return AdditiveHermite(6, [SinPeaks(1), SinPeaks(2), SinPeaks(3)], [0.0, 0.0, 0.0])
+
+
+@dataclass
+class LearnedStep:
+    xyz: torch.Tensor
+    normal: torch.Tensor
+    query: torch.Tensor
+    target: torch.Tensor
+    voxel_size: float = 1.0 / 128
+    depth: int = 3
+    min_density: float = 2.0
+    screen_alpha: float = 4.0
+    solver: str = "cholmod"
+    basis: AdditiveHermite = field(default_factory=hermite_basis)
+    tree: HashTree = None
+    sample_weight: torch.Tensor = None
+
+    def build(self):
+        """Tree and splatting weights (depend on positions only)."""
+        self.basis = self.basis.to(self.xyz.device)
+        self.tree = HashTree(self.xyz, voxel_size=self.voxel_size, depth=self.depth)
+        self.tree.build_encoder_hierarchy_adaptive(min_density=self.min_density)
+        self.tree.reflect_decoder_coords()
+        self.sample_weight = 1.0 / self.tree.xyz_density
+        return self
+
+    def init_features(self, sigma: float = 0.1, seed: int = 0) -> Dict[int, torch.Tensor]:
+        """Bezier-like initial features plus N(0, sigma) noise, per level."""
+        rng = np.random.default_rng(seed)
+        out = {}
+        for d in range(self.depth):
+            f = torch.zeros((self.tree.get_coords_size(HashTree.DECODER, d), self.basis.get_feature_size()))
+            self.basis.initialize_feature_value(f)
+            f = f + torch.from_numpy(rng.normal(0, sigma, f.shape).astype(np.float32))
+            out[d] = f.to(self.xyz.device)
+        return out
+
+    def normal_data(self, normal: torch.Tensor) -> Dict[int, torch.Tensor]:
+        t, sw = self.tree, self.sample_weight
+        out = {}
+        for d in range(t.depth):
+            m = t.xyz_depth == d
+            if not torch.any(m):
+                continue
+            nd = t.splat_data(self.xyz[m], t.DECODER, d, normal[m] * sw[m, None])
+            out[d] = nd / (t.get_stride(t.DECODER, d) ** 3)
+        return out
+
+    def forward(self, normal: torch.Tensor, feats: Dict[int, torch.Tensor]):
+        """(loss, chi at the queries, reconstructor); differentiable in ``normal`` and ``feats``."""
+        rec = Reconstructor(self.tree, self.basis, feats)
+        rec.sample_weight = self.sample_weight
+        rec.solve_multigrid(self.depth - 1, 0, self.normal_data(normal), screen_alpha=self.screen_alpha,
+                            screen_xyz=self.xyz, solver=self.solver, verbose=False)
+        chi = rec.evaluate_chi(self.query)
+        return torch.mean((chi - self.target) ** 2), chi, rec
+
+    def loss_and_grad(self, normal: torch.Tensor, feats: Dict[int, torch.Tensor]):
+        n = normal.detach().clone().requires_grad_(True)
+        f = {d: v.detach().clone().requires_grad_(True) for d, v in feats.items()}
+        loss, chi, rec = self.forward(n, f)
+        loss.backward()
+        return float(loss.detach()), n.grad, {d: v.grad for d, v in f.items()}, chi.detach(), rec

@@ -6,6 +6,7 @@ shapes, sizes and noise levels of the benchmark workloads:
 
 * ``torus``          -- 10k points, area-uniform on a torus (R=0.35, r=0.15), exact normals
 * ``superquadrics``  -- points on a union of random superquadrics, with optional noise
+* ``learned_problem``-- one noisy superquadric with query points and an analytic target field
 * ``room``           -- large indoor scene: walls, floor, ceiling and boxes / cylinders
 * ``serving_stream`` -- request sizes, depths and Poisson arrival times for the serving loop
 """
@@ -134,6 +135,23 @@ def superquadrics(n=300000, k=4, seed=0, normal_noise=0.02, pos_noise=0.002):
     if pos_noise > 0:
         xyz = xyz + rng.normal(0, pos_noise, xyz.shape)
     return xyz.astype(np.float32), nrm.astype(np.float32), shapes
+
+
+def learned_problem(n=3000, n_query=20000, seed=0, pos_noise=0.005, band=0.01):
+    """One random superquadric for the learned-basis (Neural Galerkin) training form.
+
+    Returns points (position noise ``pos_noise``), exact unit normals, query points scattered
+    around the surface (N(0, band)) and the analytic target field at the queries,
+    ``-0.1 * tanh(F(q) / 0.2)`` of the inside-outside function F (positive inside, 0 on the surface).
+    """
+    rng = np.random.default_rng(seed)
+    shape = random_superquadrics(1, rng)[0]
+    xyz, nrm, _ = shape.sample(n, rng)
+    xyz = xyz + rng.normal(0, pos_noise, xyz.shape)
+    q, _, _ = shape.sample(n_query, rng)
+    q = q + rng.normal(0, band, q.shape)
+    target = -0.1 * np.tanh(shape.inside_outside(q) / 0.2)
+    return xyz.astype(np.float32), nrm.astype(np.float32), q.astype(np.float32), target.astype(np.float32)
 
 
 def room(n=5_000_000, seed=0, size=(8.0, 8.0, 3.0), n_objects=40, noise=0.005):

@@ -19,7 +19,9 @@ ops are CUDA-only pybind11 modules, and ``jittor``, ``torch_scatter`` and
 Everything the reference computes in torch (trilinear weights, quantisation,
 neighbour queries, density, levels, RHS / LHS assembly, correction, chi,
 conformal tree, dual-grid construction, vertex de-duplication) is the
-reference's own code.  Run from the repository root:
+reference's own code.  The learned-basis case also writes the reference's additive-integral cache files (which it
+would otherwise compute with sympy) from its own symbolic components.  Run from the
+repository root (``python tests/golden/make_golden.py [tables|learned|<case>...]``):
 
     python tests/golden/make_golden.py
 """
@@ -300,14 +302,159 @@ def range_kernel_case():
                         keys4=O.hash_cuda(np.concatenate([coords, coords[:, :1]], 1)))
 
 
+LEARNED = dict(seed=0, voxel_size=1.0 / 128, depth=3, min_density=2.0, screen_alpha=4.0, feat_sigma=0.1)
+
+
+def _learned_components():
+    """The learned basis of ``configs/shapenet/full_net_base.yaml:54-59`` as the reference builds it."""
+    from jspsr.bases import additive_components as AC
+    comps = [AC.SinPeaks(1), AC.SinPeaks(2), AC.SinPeaks(3)]
+    return comps + [AC.Power(p) for p in range(7)]
+
+
+def additive_tables_case(n_mult: int = 5):
+    """theta / rho tables of the learned basis's ten components from the reference's symbolic
+    definitions (``additive.py:17-52``), integrated with adaptive quadrature, written as the
+    reference's own cache files (``additive.py:178-246``) and as a fixture.
+
+    sympy's piecewise integration of these products does not finish here, so the reference's
+    symbolic components are lambdified and integrated with scipy ``quad`` over the same intervals
+    and index conventions."""
+    import sympy as sp
+    from scipy.integrate import quad
+    import jspsr
+    comps = _learned_components()
+    x = sp.Symbol("x")
+    fs = [sp.lambdify(x, c.symbolic(x), "math") for c in comps]
+    dfs = [sp.lambdify(x, sp.diff(c.symbolic(x), x), "math") for c in comps]
+    brk = [-1.5, 1.5]
+
+    def integ(fn, lo, hi, pts):
+        if hi <= lo:
+            return 0.0
+        pts = sorted(p for p in set(pts) if lo < p < hi)
+        return quad(fn, lo, hi, points=pts or None, limit=200, epsabs=1e-14, epsrel=1e-13)[0]
+
+    def objarr(lists):
+        a = np.empty(len(lists), dtype=object)
+        for i, v in enumerate(lists):
+            a[i] = [float(t) for t in v]
+        return a
+
+    cache = Path(jspsr.__file__).parent / "data" / "additive_integrals"
+    cache.mkdir(parents=True, exist_ok=True)
+    fixture = {}
+    C = len(comps)
+    for a in range(C):
+        for b in range(C):
+            ff, dd = [], []
+            for m in range(n_mult):
+                M = 2 ** m
+                rf, rd = [], []
+                for dx in np.arange(-1.5 * M - 0.5, 1.5 * M + 1.5):
+                    lo, hi = max(-1.5 - dx, -1.5 * M), min(1.5 - dx, 1.5 * M)
+                    pts = [q - dx for q in brk] + [q * M for q in brk] + [0.0]
+                    rf.append(integ(lambda y: fs[a](y + dx) * fs[b](y / M), lo, hi, pts))
+                    rd.append(integ(lambda y: dfs[a](y + dx) * dfs[b](y / M) / M, lo, hi, pts))
+                ff.append(rf)
+                dd.append(rd)
+                fixture[f"ff_{a}_{b}_{m}"] = np.asarray(rf)
+                fixture[f"dfdf_{a}_{b}_{m}"] = np.asarray(rd)
+            np.savez_compressed(cache / f"ff-{comps[a]}-{comps[b]}.npz", f_f=objarr(ff), df_df=objarr(dd))
+    for a in range(C):
+        f, df, fi, dfi = [], [], [], []
+        for m in range(n_mult):
+            M = 2 ** m
+            rf, rd = [], []
+            for ra in np.arange(-1.5 * M, 1.5 * M):
+                rf.insert(0, integ(lambda y: fs[a](y / M), ra, ra + 1, [q * M for q in brk]))
+                rd.insert(0, integ(lambda y: dfs[a](y / M) / M, ra, ra + 1, [q * M for q in brk]))
+            f.append(rf)
+            df.append(rd)
+            fixture[f"f_{a}_{m}"], fixture[f"df_{a}_{m}"] = np.asarray(rf), np.asarray(rd)
+        for m in range(1, n_mult):
+            M = 2 ** m
+            rf, rd = [], []
+            for ra in np.arange(-M - 0.5, 1.5):
+                lb, ub = max(ra, -1.5), min(ra + M, 1.5)
+                rf.insert(0, integ(fs[a], lb, ub, brk))
+                rd.insert(0, integ(dfs[a], lb, ub, brk))
+            fi.append(rf)
+            dfi.append(rd)
+            fixture[f"finv_{a}_{m}"], fixture[f"dfinv_{a}_{m}"] = np.asarray(rf), np.asarray(rd)
+        np.savez_compressed(cache / f"f-{comps[a]}.npz", f=objarr(f), df=objarr(df), f_inv=objarr(fi),
+                            df_inv=objarr(dfi))
+    fixture["names"] = np.array([repr(c) for c in comps])
+    np.savez_compressed(HERE / "additive_tables.npz", **fixture)
+    print("additive tables", len(fixture))
+
+
+def learned_case():
+    """The Neural Galerkin training form on the reference's own classes: AdditiveHermite basis with
+    per-voxel features (Bezier-like initialisation + N(0, 0.1)), density-adaptive tree, normals
+    splatted as ``jspsr/__init__.py:36-47`` does, multigrid solve with screening, loss = MSE of
+    ``evaluate_chi`` at query points against an analytic target; gradients by the reference's
+    autograd graph (its DDIFunc / EvalFunc / ScreenedMultiplication / Solver backward)."""
+    from jspsr.core.hashtree import HashTree
+    from jspsr.core.reconstructor import Reconstructor
+    from jspsr.bases.hermite_ns import AdditiveHermite
+    from jspsr.bases import additive_components as AC
+    P = LEARNED
+    xyz, nrm, q, target = synthetic.learned_problem(seed=P["seed"])
+    xyz_t = torch.from_numpy(xyz)
+    nrm_t = torch.from_numpy(nrm).requires_grad_(True)
+    basis = AdditiveHermite(6, [AC.SinPeaks(1), AC.SinPeaks(2), AC.SinPeaks(3)], [0.0, 0.0, 0.0])
+    ht = HashTree(xyz_t, voxel_size=P["voxel_size"], depth=P["depth"])
+    ht.build_encoder_hierarchy_adaptive(min_density=P["min_density"])
+    ht.reflect_decoder_coords()
+    sw = 1.0 / ht.xyz_density
+    normal_data = {}
+    for d in range(ht.depth):
+        msk = ht.xyz_depth == d
+        if not torch.any(msk):
+            continue
+        nd = ht.splat_data(xyz_t[msk], ht.DECODER, d, nrm_t[msk] * sw[msk, None])
+        normal_data[d] = nd / (ht.get_stride(ht.DECODER, d) ** 3)
+    rng = np.random.default_rng(P["seed"] + 7)
+    feats = {}
+    for d in range(ht.depth):
+        f0 = torch.zeros((ht.get_coords_size(ht.DECODER, d), basis.get_feature_size()))
+        basis.initialize_feature_value(f0)
+        f0 = f0 + torch.from_numpy(rng.normal(0, P["feat_sigma"], f0.shape).astype(np.float32))
+        feats[d] = f0.requires_grad_(True)
+    rec = Reconstructor(ht, basis, feats)
+    rec.sample_weight = sw
+    rec.solve_multigrid(ht.depth - 1, 0, normal_data, screen_alpha=P["screen_alpha"], screen_xyz=xyz_t,
+                        solver="cholmod", verbose=False)
+    chi = rec.evaluate_chi(torch.from_numpy(q))
+    loss = torch.mean((chi - torch.from_numpy(target)) ** 2)
+    loss.backward()
+    out = dict(xyz=xyz, nrm=nrm, query=q, target=target,
+               params=np.array([P["voxel_size"], P["depth"], P["min_density"], P["screen_alpha"]]),
+               density=ht.xyz_density.numpy(), levels=ht.xyz_depth.numpy(), chi=chi.detach().numpy(),
+               loss=np.array(float(loss)), grad_nrm=nrm_t.grad.numpy())
+    for d in range(ht.depth):
+        out[f"coords{d}"] = ht.get_coords(ht.DECODER, d).numpy()
+        out[f"feat{d}"] = feats[d].detach().numpy()
+        out[f"grad_feat{d}"] = feats[d].grad.numpy()
+        out[f"x{d}"] = rec.solutions[d].detach().numpy()
+    np.savez_compressed(HERE / "learned_sq.npz", **out)
+    print("learned", float(loss), {k: v.shape for k, v in out.items() if k.startswith(("coords", "grad"))})
+
+
 def main():
     _prepare_reference()
-    tables_case()
-    mc_tables_case()
-    range_kernel_case()
-    names = sys.argv[1:] or list(CASES)
-    for n in names:
-        run_case(n, *CASES[n])
+    names = sys.argv[1:]
+    if not names or "tables" in names:
+        tables_case()
+        mc_tables_case()
+        range_kernel_case()
+    if not names or "learned" in names:
+        additive_tables_case()
+        learned_case()
+    for n in names or list(CASES):
+        if n in CASES:
+            run_case(n, *CASES[n])
 
 
 if __name__ == "__main__":
