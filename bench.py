@@ -31,15 +31,35 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "neural-galerkin_b200"))
 
-WORKLOAD = dict(workload="superquadrics-300k", n_points=300000, n_shapes=4, seed=0, voxel_size=1.0 / 512,
-                depth=4, min_density=2.0, screen_alpha=4.0, solver="pcg-mixed@tol=1e-7")
+WORKLOADS = {
+    # the headline workload (one step = one reconstruction)
+    "superquadrics-300k": dict(workload="superquadrics-300k", n_points=300000, n_shapes=4, seed=0,
+                               voxel_size=1.0 / 512, depth=4, min_density=2.0, screen_alpha=4.0,
+                               solver="pcg-mixed@tol=1e-7"),
+    # the same kind of cloud at a third of the size (profiling captures)
+    "superquadrics-100k": dict(workload="superquadrics-100k", n_points=100000, n_shapes=4, seed=0,
+                               voxel_size=1.0 / 512, depth=4, min_density=0.7, screen_alpha=4.0,
+                               solver="pcg-mixed@tol=1e-7"),
+    # 10k points on a torus, 3 levels at 1/128
+    "torus-10k": dict(workload="torus-10k", n_points=10000, n_shapes=0, seed=0, voxel_size=1.0 / 128, depth=3,
+                      min_density=1.5, screen_alpha=4.0, solver="pcg-mixed@tol=1e-7"),
+    # 5M points in an 8 x 8 x 3 m room, 1 cm voxels, 11 levels
+    "room-5m": dict(workload="room-5m", n_points=5_000_000, n_shapes=40, seed=0, voxel_size=0.01, depth=11,
+                    min_density=2.0, screen_alpha=4.0, solver="pcg-mixed@tol=1e-7"),
+}
+WORKLOAD = dict(WORKLOADS["superquadrics-300k"])
 PLAIN_SOLVER = "plain-fp64@tol=1e-7"
 FP64_SOLVER = "pcg-fp64@tol=1e-12"
 
 
 def workload_points():
     from jspsr import synthetic
-    xyz, nrm, _ = synthetic.superquadrics(WORKLOAD["n_points"], k=WORKLOAD["n_shapes"], seed=WORKLOAD["seed"])
+    W = WORKLOAD
+    if W["workload"].startswith("torus"):
+        return synthetic.torus(n=W["n_points"], seed=W["seed"])
+    if W["workload"].startswith("room"):
+        return synthetic.room(n=W["n_points"], seed=W["seed"], n_objects=W["n_shapes"])
+    xyz, nrm, _ = synthetic.superquadrics(W["n_points"], k=W["n_shapes"], seed=W["seed"])
     return xyz, nrm
 
 
@@ -122,6 +142,100 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- learned-basis leg
+def learned_leg(n_shapes=32):
+    """Neural Galerkin forward + adjoint on ``n_shapes`` random superquadrics (3,000 points, voxel
+    1/128, 3 levels, AdditiveHermite basis with 18 features per voxel ~ init + N(0, 0.1), loss = MSE of
+    chi at 20,000 queries against the analytic target): device time per shape."""
+    import torch
+    from jspsr import synthetic
+    from jspsr.core.learned import LearnedStep
+    fw, bw, loss = [], [], []
+    voxels = []
+    for seed in range(n_shapes + 1):
+        xyz, nrm, q, tgt = synthetic.learned_problem(seed=seed)
+        T = lambda a: torch.from_numpy(a).cuda()     # noqa: E731
+        s = LearnedStep(T(xyz), T(nrm), T(q), T(tgt), min_density=None).build()
+        feats = s.init_features(0.1, seed=seed)
+        n = s.normal.clone().requires_grad_(True)
+        f = {d: v.clone().requires_grad_(True) for d, v in feats.items()}
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        lo, _, _ = s.forward(n, f)
+        e[1].record()
+        lo.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        if seed == 0:
+            continue                     # first shape: warm-up (table upload, allocator)
+        fw.append(e[0].elapsed_time(e[1]))
+        bw.append(e[1].elapsed_time(e[2]))
+        loss.append(float(lo))
+        voxels.append(sum(s.tree.get_coords_size(s.tree.DECODER, d) for d in range(s.depth)))
+    return {"shapes": n_shapes, "forward_ms_per_shape": float(np.mean(fw)), "adjoint_ms_per_shape": float(np.mean(bw)),
+            "shapes_per_s": 1e3 / float(np.mean(np.add(fw, bw))), "mean_voxels": float(np.mean(voxels)),
+            "config": "3,000 points + N(0,0.005) on a random superquadric, voxel 1/128, 3 levels, "
+                      "AdditiveHermite(6, SinPeaks(1..3)) 18 features/voxel, 20,000 queries, cholmod-equivalent "
+                      "FP64-refined solves forward and adjoint; gradients w.r.t. normals and features"}
+
+
+# ----------------------------------------------------------------------------- serving leg
+def serving_leg(n_requests=1024, slots=8, plain_every=8):
+    """1,024 requests (points log-uniform in [1e3, 5e5], superquadric/torus unions, N(0,0.003) noise,
+    finest voxel 2^-U{6..9}, 4 levels), Poisson arrivals at 200/s; host payloads in pinned memory,
+    meshes back to pinned memory.  Compares the continuous-batching server against one request at
+    a time (latency = service time alone)."""
+    import torch
+    from jspsr import synthetic
+    from jspsr.serving import Request, ReconServer, run_sequential, latency_stats
+    descs = synthetic.serving_stream(n_requests=n_requests)
+    reqs = []
+    for i, dsc in enumerate(descs):
+        x, n = synthetic.serving_request_device(dsc, "cuda")
+        reqs.append(Request(x.cpu().pin_memory(), n.cpu().pin_memory(), 2.0 ** -dsc["finest_depth"], depth=4,
+                            arrival=dsc["arrival"], rid=i))
+    torch.cuda.synchronize()
+    run_sequential(reqs[:8], keep_meshes=False)                 # warm-up
+    seq = run_sequential(reqs, keep_meshes=False)
+    seq_s = seq[-1].done - seq[0].arrival
+    sub = reqs[::plain_every]
+    seq_plain = run_sequential(sub, solver="plain-fp64@tol=1e-7", keep_meshes=False)
+    t_plain = sum(r.latency for r in seq_plain)
+    t_mixed_sub = sum(seq[i].latency for i in range(0, n_requests, plain_every))
+    plain_rps = n_requests / (seq_s * t_plain / t_mixed_sub)
+    srv = ReconServer(slots=slots, keep_meshes=False)
+    try:
+        srv.run(reqs[:32], realtime=False)                      # warm-up (streams, allocator pools)
+        l0, s0 = srv.batcher.launches, srv.batcher.batched_systems
+        rt = srv.run(reqs, realtime=True)
+        rt_s = max(r.done for r in rt) - min(r.arrival for r in rt)
+        l1, s1 = srv.batcher.launches, srv.batcher.batched_systems
+        sat = srv.run(reqs, realtime=False)
+        sat_s = max(r.done for r in sat)
+        waits, peak = srv.adm.waits, srv.adm.peak_in_use
+    finally:
+        srv.close()
+    errors = sum(r.error is not None for r in rt + sat)
+    seq_rps = n_requests / seq_s
+    rt_stats, alone = latency_stats(rt), latency_stats(seq)
+    return {"requests": n_requests, "slots": slots, "errors": errors,
+            "offered_rate_rps": 200.0,
+            "served_recon_per_s_at_offered_rate": n_requests / rt_s,
+            "p50_ms": rt_stats["p50_ms"], "p99_ms": rt_stats["p99_ms"],
+            "saturated_recon_per_s": n_requests / sat_s,
+            "saturated": latency_stats(sat),
+            "sequential_recon_per_s": seq_rps, "sequential_alone_latency": alone,
+            "sequential_plain_fp64_recon_per_s": plain_rps,
+            "plain_fp64_sample": f"every {plain_every}th request ({len(sub)}), scaled by the mixed-solver time of the same requests",
+            "speedup_vs_sequential": (n_requests / sat_s) / seq_rps,
+            "speedup_vs_sequential_plain_fp64": (n_requests / sat_s) / plain_rps,
+            "p99_over_alone_p99": rt_stats["p99_ms"] / alone["p99_ms"],
+            "pcg_launches_per_system": (l1 - l0) / max(1, s1 - s0),
+            "admission_waits": waits, "peak_admitted_bytes": int(peak),
+            "total_points": int(sum(r.xyz.shape[0] for r in reqs))}
+
+
 # ----------------------------------------------------------------------------- our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -131,8 +245,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-comparators", action="store_true")
+    ap.add_argument("--workload", default="superquadrics-300k", choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", default="all", choices=["all", "recon", "learned", "serving"],
+                    help="all: reconstruction line with the learned-basis and serving legs attached")
+    ap.add_argument("--serving-requests", type=int, default=1024)
+    ap.add_argument("--learned-shapes", type=int, default=32)
+    ap.add_argument("--serving-slots", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    WORKLOAD.clear()
+    WORKLOAD.update(WORKLOADS[args.workload])
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -151,6 +273,14 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     lib = L.load()
+    if args.mode in ("learned", "serving"):
+        leg = learned_leg(args.learned_shapes) if args.mode == "learned" else \
+            serving_leg(args.serving_requests, slots=args.serving_slots)
+        if rank == 0:
+            print(json.dumps({"mode": args.mode, **leg}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     xyz, nrm = workload_points()
     X = torch.from_numpy(xyz).cuda()
     N = torch.from_numpy(nrm).cuda()
@@ -250,14 +380,31 @@ def main():
         c1.record()
         torch.cuda.synchronize()
         plain_ms = c0.elapsed_time(c1) / 2
-        ref64, _, _ = step(solver=FP64_SOLVER)
+        plain_rec, _, _ = step(solver=PLAIN_SOLVER, profile=True)
+        plain_solve = plain_rec.pcg_ms
+        plain_iters = {d: int(lv.info[0]) for d, lv in enumerate(plain_rec.levels)}
+        ref64, _, _ = step(solver=FP64_SOLVER, profile=True)
+        fp64_solve = ref64.pcg_ms
         chi = rec.chi_raw(X) - rec.mean_chi()
         chi64 = ref64.chi_raw(X) - ref64.mean_chi()
         err = float(torch.linalg.norm(chi.double() - chi64.double()) / torch.linalg.norm(chi64.double()))
+        xerr = max(float(torch.linalg.norm(a.x64 - b.x64) / torch.linalg.norm(b.x64))
+                   for a, b in zip(rec.levels, ref64.levels))
+        mixed_solve = sum(pcg_ms.values())
         extra = {"plain_fp64_ms_per_step": plain_ms, "speedup_vs_plain_fp64": plain_ms / (ms / args.steps),
-                 "field_rel_err_vs_fp64_solve": err,
+                 "solve_ms": {"mixed": mixed_solve, "plain_fp64_host_driven": sum(plain_solve.values()),
+                              "fp64_persistent": sum(fp64_solve.values())},
+                 "solve_speedup_vs_plain_fp64": sum(plain_solve.values()) / mixed_solve,
+                 "solve_speedup_vs_fp64_persistent": sum(fp64_solve.values()) / mixed_solve,
+                 "field_rel_err_vs_fp64_solve": err, "solution_rel_err_vs_fp64_solve": xerr,
                  "pcg_ms_per_level": pcg_ms, "pcg_iters_per_level": {d: s["iters"] for d, s in stats.items()},
+                 "plain_fp64_iters_per_level": plain_iters,
                  "mesh": {"vertices": int(v.shape[0]), "faces": int(f.shape[0])}}
+
+    # ---------------------------------------------------------------- learned-basis and serving legs
+    if args.mode == "all" and rank == 0 and world == 1:
+        extra["learned"] = learned_leg(args.learned_shapes)
+        extra["serving"] = serving_leg(args.serving_requests, slots=args.serving_slots)
 
     # ---------------------------------------------------------------- CPU baseline (oracle on a bounded sample)
     cpu = None

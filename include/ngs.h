@@ -233,6 +233,27 @@ size_t ngs_pcg_workspace_bytes(int64_t n, int mode);
 int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
                   int64_t* info_dev, double* resid_dev, ngs_stream s);
 
+/* Several independent systems in ONE cooperative launch (the serving path's batched solve; no
+ * counterpart in the reference).  Every system keeps the block count a single ngs_pcg_solve of it
+ * would use (ngs_pcg_blocks), so its tile plan and reduction order -- and therefore its result,
+ * bit for bit -- are those of solving it alone; its status, iterations and residual land in its own
+ * info_dev / resid_dev.  All items share one mode; at most NGS_PCG_BATCH_MAX items; the blocks of
+ * all non-empty items must fit ngs_pcg_block_capacity(mode) (co-residency of a cooperative launch),
+ * otherwise NGS_ERR_INVALID_ARG and nothing is launched -- split the batch.  Each item needs its own
+ * workspace of ngs_pcg_workspace_bytes(n, mode) bytes. */
+#define NGS_PCG_BATCH_MAX 64
+typedef struct ngs_pcg_batch_item {
+  ngs_pcg_system sys;
+  ngs_pcg_config cfg;
+  void* ws;
+  size_t ws_bytes;
+  int64_t* info_dev;         /* int64[4], as ngs_pcg_solve */
+  double* resid_dev;         /* double[2] */
+} ngs_pcg_batch_item;
+int ngs_pcg_block_capacity(int mode);
+int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode);
+int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items, ngs_stream s);
+
 /* ngs_pcg_solve without any workspace from the caller, for callers that cannot allocate device
  * memory when they solve (no counterpart in the reference).  Scratch lives in a static device
  * array inside the library, sized for n <= ngs_pcg_noalloc_max_rows() (131072) rows; larger

@@ -258,23 +258,70 @@ __global__ void vd_scatter_kernel(const int32_t* __restrict__ vids, int64_t n, c
   }
 }
 
-// Sort each bucket by (vid1, key index) and flag the first key of every distinct vid1.
+// Sort each bucket by (vid1, key index) and flag the first key of every distinct vid1.  One warp
+// per bucket: the keys of a bucket are distinct (the low half is the key's index), so each key's
+// position is the number of keys below it, counted by broadcasting the bucket through the warp
+// 32 keys at a time; then every lane writes its keys straight to their positions.  K keys per lane
+// live in registers, so the warp sorts buckets of up to 32 K keys; K is picked per bucket.
+template <int K>
+NGS_DEV void vd_rank_sort(int64_t s0, int c, int lane, int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
+  int64_t mine[K];
+  int rank[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const int idx = lane + 32 * k;
+    mine[k] = idx < c ? sorted[s0 + idx] : INT64_MAX;
+    rank[k] = 0;
+  }
+  const int nchunks = (c + 31) / 32;
+  for (int chunk = 0; chunk < nchunks; chunk++) {
+    const int64_t other = chunk * 32 + lane < c ? sorted[s0 + chunk * 32 + lane] : INT64_MAX;
+    const int lim = min(32, c - chunk * 32);
+    for (int j = 0; j < lim; j++) {
+      const int64_t o = __shfl_sync(0xffffffffu, other, j);
+#pragma unroll
+      for (int k = 0; k < K; k++) rank[k] += o < mine[k] ? 1 : 0;
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (lane + 32 * k < c) sorted[s0 + rank[k]] = mine[k];
+  __syncwarp();
+  for (int i = lane; i < c; i += 32)
+    first[s0 + i] = (i == 0 || (sorted[s0 + i] >> 32) != (sorted[s0 + i - 1] >> 32)) ? 1 : 0;
+  __syncwarp();
+}
+
 __global__ void vd_sort_kernel(const int64_t* __restrict__ start, const int32_t* __restrict__ count, int64_t nb,
                                int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
-  for (int64_t b = ngs_gtid(); b < nb; b += ngs_gstride()) {
-    const int64_t s0 = start[b];
+  const int lane = threadIdx.x & 31;
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b = warp0; b < nb; b += nwarps) {
     const int c = count[b];
-    for (int i = 1; i < c; i++) {
-      const int64_t key = sorted[s0 + i];
-      int j = i - 1;
-      while (j >= 0 && sorted[s0 + j] > key) {
-        sorted[s0 + j + 1] = sorted[s0 + j];
-        j--;
-      }
-      sorted[s0 + j + 1] = key;
+    if (c <= 1) {
+      if (c == 1 && lane == 0) first[start[b]] = 1;
+      continue;
     }
-    for (int i = 0; i < c; i++)
-      first[s0 + i] = (i == 0 || (sorted[s0 + i] >> 32) != (sorted[s0 + i - 1] >> 32)) ? 1 : 0;
+    const int64_t s0 = start[b];
+    if (c <= 32) vd_rank_sort<1>(s0, c, lane, sorted, first);
+    else if (c <= 128) vd_rank_sort<4>(s0, c, lane, sorted, first);
+    else if (c <= 512) vd_rank_sort<16>(s0, c, lane, sorted, first);
+    else if (lane == 0) {
+      // bucket beyond 512 keys (not produced by the dual grids here): serial insertion sort
+      for (int i = 1; i < c; i++) {
+        const int64_t key = sorted[s0 + i];
+        int j = i - 1;
+        while (j >= 0 && sorted[s0 + j] > key) {
+          sorted[s0 + j + 1] = sorted[s0 + j];
+          j--;
+        }
+        sorted[s0 + j + 1] = key;
+      }
+      for (int i = 0; i < c; i++)
+        first[s0 + i] = (i == 0 || (sorted[s0 + i] >> 32) != (sorted[s0 + i - 1] >> 32)) ? 1 : 0;
+    }
   }
 }
 
@@ -317,7 +364,7 @@ extern "C" int ngs_vdedup_sort(const int32_t* vert_ids, int64_t n_keys, const in
   if (n_keys == 0) return NGS_OK;
   cudaStream_t st = (cudaStream_t)s;
   { ngs_count_launch(); vd_scatter_kernel<<<ngs_blocks(n_keys, 256), 256, 0, st>>>(vert_ids, n_keys, bucket_start, bucket_fill, sorted_keys); }
-  { ngs_count_launch(); vd_sort_kernel<<<ngs_blocks(n_buckets, 128), 128, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
+  { ngs_count_launch(); vd_sort_kernel<<<ngs_blocks(n_buckets * 32, 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

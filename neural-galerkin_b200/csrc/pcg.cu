@@ -131,13 +131,13 @@ NGS_DEV int64_t first_row_at(const int64_t* __restrict__ rp, int64_t n, int64_t 
 // PCG_TILE_ROWS rows.  Rows longer than PCG_MAX_ROW, or empty, are rejected.  Returns false for such a block.
 constexpr int PCG_MAX_ROW = 250;
 
-NGS_DEV bool plan_tiles(const PcgArgs& a, BlockRows& br) {
+NGS_DEV bool plan_tiles(const PcgArgs& a, unsigned bid, BlockRows& br) {
   __shared__ int64_t bounds[2];
   __shared__ int nt, bad;
   if (threadIdx.x == 0) {
     const int64_t B = a.nblocks;
-    bounds[0] = first_row_at(a.rowptr, a.n, (a.nnz * (int64_t)blockIdx.x) / B);
-    bounds[1] = blockIdx.x + 1 == a.nblocks ? a.n : first_row_at(a.rowptr, a.n, (a.nnz * ((int64_t)blockIdx.x + 1)) / B);
+    bounds[0] = first_row_at(a.rowptr, a.n, (a.nnz * (int64_t)bid) / B);
+    bounds[1] = bid + 1 == a.nblocks ? a.n : first_row_at(a.rowptr, a.n, (a.nnz * ((int64_t)bid + 1)) / B);
     nt = 0;
     bad = 0;
   }
@@ -264,7 +264,7 @@ NGS_DEV bool spmv_tiles(const PcgArgs& a, const MT* __restrict__ vals, const VT*
 
 // Block sums of NV doubles -> per-block partials -> fixed-order grid reduction.
 template <int NV>
-NGS_DEV bool reduce_barrier(const PcgArgs& a, const double (&v)[NV], double (&out)[NV]) {
+NGS_DEV bool reduce_barrier(const PcgArgs& a, unsigned bid, const double (&v)[NV], double (&out)[NV]) {
   __shared__ double red[NV > 0 ? NV : 1][PCG_THREADS / 32];
   __shared__ int last, ok;
   __shared__ unsigned int gen0;
@@ -281,7 +281,7 @@ NGS_DEV bool reduce_barrier(const PcgArgs& a, const double (&v)[NV], double (&ou
     for (int k = 0; k < NV; k++) {
       double t = 0.0;
       for (int i = 0; i < PCG_THREADS / 32; i++) t += red[k][i];
-      a.partials[(size_t)blockIdx.x * 4 + k] = t;
+      a.partials[(size_t)bid * 4 + k] = t;
     }
     gen0 = *reinterpret_cast<volatile unsigned int*>(a.gen);
     __threadfence();
@@ -332,9 +332,9 @@ NGS_DEV bool reduce_barrier(const PcgArgs& a, const double (&v)[NV], double (&ou
   return ok != 0;
 }
 
-NGS_DEV bool plain_barrier(const PcgArgs& a) {
+NGS_DEV bool plain_barrier(const PcgArgs& a, unsigned bid) {
   double v[1] = {0.0}, o[1];
-  return reduce_barrier<1>(a, v, o);
+  return reduce_barrier<1>(a, bid, v, o);
 }
 
 NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0; }
@@ -352,8 +352,10 @@ constexpr size_t pcg_smem_bytes(int mode) {
          ((PCG_TILE_ROWS + 4) * 4 + 15) / 16 * 16 + 2 * (PCG_MAX_TILES + 4) * 4 + 64;
 }
 
+// The solve of one system by the blocks bid = 0 .. a.nblocks-1 of a launch (all of them for a
+// single solve, a contiguous range for one system of a batch).
 template <int MODE>
-__global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
+NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
   using MT = typename PcgTypes<MODE>::MT;
   using VT = typename PcgTypes<MODE>::VT;
   using RT = typename PcgTypes<MODE>::RT;
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
     mbar_fence_init();
   }
   __syncthreads();
-  const bool rows_ok = plan_tiles(a, br);
+  const bool rows_ok = plan_tiles(a, bid, br);
   const int64_t i0 = br.row0 + threadIdx.x, i1 = br.row1, is = PCG_THREADS;
 
   // w = A u; returns (w, u).  The row's u is prefetched during the tile's product pass.
@@ -428,9 +430,9 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
     s[i] = (VT)0;
     part[0] += (double)bi * (double)bi;
   }
-  if (!reduce_barrier<3>(a, part, res)) return;
+  if (!reduce_barrier<3>(a, bid, part, res)) return;
   if (res[1] > 0.0) {                                    // every block sees the same flag: no copy was issued
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bid == 0 && threadIdx.x == 0) {
       a.info[0] = 0;
       a.info[1] = NGS_ERR_INVALID_ARG;
     }
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
     part[0] += (double)r[i] * (double)u[i];
     part[2] += (double)r[i] * (double)r[i];
   }
-  if (!reduce_barrier<3>(a, part, res)) return;
+  if (!reduce_barrier<3>(a, bid, part, res)) return;
   double gamma = res[0], delta = res[1], rho = res[2];
   double alpha = delta != 0.0 ? gamma / delta : 0.0, beta = 0.0;
   int it = 0, replacements = 0;
@@ -477,17 +479,17 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
     }
     if (replace) {
       // residual replacement: r = b - A x (FP64 matrix in MIXED mode, the FP32 one in REFERENCE mode)
-      if (!plain_barrier(a)) return;
+      if (!plain_barrier(a, bid)) return;
       double rr = 0.0;
       if (!spmv_true(rr)) return;
       part[2] = rr;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       replacements++;
     }
-    if (!plain_barrier(a)) return;
+    if (!plain_barrier(a, bid)) return;
     // phase B: w = A u and (w, u)
     if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
-    if (!reduce_barrier<3>(a, part, res)) return;
+    if (!reduce_barrier<3>(a, bid, part, res)) return;
     it++;
     const double gamma_new = res[0];
     delta = res[1];
@@ -495,14 +497,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
     if (sqrt(rho) <= target) {
       if (MODE != NGS_PCG_MIXED) { converged = true; break; }
       // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
-      if (!plain_barrier(a)) return;
+      if (!plain_barrier(a, bid)) return;
       part[0] = part[1] = part[2] = 0.0;
       if (!spmv_true(part[2])) return;
       replacements++;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
-      if (!plain_barrier(a)) return;
+      if (!plain_barrier(a, bid)) return;
       if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
-      if (!reduce_barrier<3>(a, part, res)) return;
+      if (!reduce_barrier<3>(a, bid, part, res)) return;
       rho = res[2];
       if (sqrt(rho) <= atol) { converged = true; break; }
       gamma = res[0];
@@ -519,13 +521,39 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(PcgArgs a) {
   }
   if (a.x32_out)
     for (int64_t i = i0; i < i1; i += is) a.x32_out[i] = (float)x[i];
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     a.info[0] = it;
     a.info[1] = converged ? NGS_OK : (timed_out ? NGS_ERR_TIMEOUT : NGS_ERR_NOT_CONVERGED);
     a.info[2] = replacements;
     a.resid[0] = sqrt(rho);
     a.resid[1] = bnorm;
   }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(const __grid_constant__ PcgArgs a) {
+  pcg_body<MODE>(a, blockIdx.x);
+}
+
+// A batch of independent systems in one cooperative launch: system k owns the blocks
+// [start[k], start[k+1]), with the block count its single solve would use, so that its tile plan,
+// its reductions and therefore its result are bit-identical to solving it alone.  Every system has
+// its own workspace, barrier counters, deadline and status.
+struct PcgBatch {
+  PcgArgs sys[NGS_PCG_BATCH_MAX];
+  unsigned int start[NGS_PCG_BATCH_MAX + 1];
+  int nsys;
+};
+static_assert(sizeof(PcgBatch) <= 32000, "batch arguments must fit the kernel parameter space");
+
+template <int MODE>
+__global__ void __launch_bounds__(PCG_THREADS, 1) pcg_batch_kernel(const __grid_constant__ PcgBatch b) {
+  int lo = 0, hi = b.nsys - 1;              // last system whose first block is <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.start[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
+  }
+  pcg_body<MODE>(b.sys[lo], blockIdx.x - b.start[lo]);
 }
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -539,36 +567,56 @@ extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
   return bytes;
 }
 
+// Blocks one solve uses: as many co-resident blocks as fit, fewer for small systems (about one
+// tile of work each); 0 if the system is too large for the tile plan.
 template <int MODE>
-static int launch_pcg(PcgArgs& a, int blocks_req, cudaStream_t st) {
+static int pcg_capacity() {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = pcg_smem_bytes(MODE);
-  cudaError_t e = cudaFuncSetAttribute(pcg_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  if (cudaFuncSetAttribute(pcg_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(pcg_batch_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+    return 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, smem);
-  if (per_sm < 1) return NGS_ERR_CUDA;
-  int64_t blocks = (int64_t)sms * per_sm;
-  // small systems: fewer blocks, each with at least a few tiles of work
-  const int64_t need = (a.nnz + (int64_t)PCG_ROW_COST * a.n + 4 * PCG_TILE_BODY - 1) / (4 * PCG_TILE_BODY);
-  if (blocks > need) blocks = need > 0 ? need : 1;
-  // a block owns at most PCG_MAX_TILES tiles
-  if ((a.nnz + (int64_t)PCG_ROW_COST * a.n) / blocks + 512 > (int64_t)(PCG_MAX_TILES - 2) * PCG_TILE_BODY)
-    return NGS_ERR_INVALID_ARG;
-  if (blocks_req > 0 && blocks_req < blocks) blocks = blocks_req;
-  if (blocks > 148 * 32) blocks = 148 * 32;
-  a.nblocks = (unsigned int)blocks;
-  void* args[] = {&a};
-  ngs_count_launch();
-  e = cudaLaunchCooperativeKernel((const void*)pcg_kernel<MODE>, dim3((unsigned)blocks), dim3(PCG_THREADS), args,
-                                  smem, st);
-  if (e != cudaSuccess) return ngs_set_cuda_error(e);
-  return NGS_OK;
+  const int64_t cap = (int64_t)sms * per_sm;
+  return (int)(cap < 148 * 32 ? cap : 148 * 32);
 }
 
-extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
-                             int64_t* info_dev, double* resid_dev, ngs_stream s) {
+static int64_t pcg_blocks_for(int64_t n, int64_t nnz, int blocks_req, int capacity) {
+  int64_t blocks = capacity;
+  // one tile of work per block when the system is small: the iteration's critical path is then one
+  // staged tile plus the two grid barriers
+  const int64_t need = (nnz + (int64_t)PCG_ROW_COST * n + PCG_TILE_BODY - 1) / PCG_TILE_BODY;
+  if (blocks > need) blocks = need > 0 ? need : 1;
+  if (blocks_req > 0 && blocks_req < blocks) blocks = blocks_req;
+  if (blocks < 1) return 0;
+  // a block owns at most PCG_MAX_TILES tiles
+  if ((nnz + (int64_t)PCG_ROW_COST * n) / blocks + 512 > (int64_t)(PCG_MAX_TILES - 2) * PCG_TILE_BODY) return 0;
+  return blocks;
+}
+
+static int capacity_of(int mode) {
+  if (mode == NGS_PCG_REFERENCE) return pcg_capacity<NGS_PCG_REFERENCE>();
+  if (mode == NGS_PCG_MIXED) return pcg_capacity<NGS_PCG_MIXED>();
+  return pcg_capacity<NGS_PCG_FP64>();
+}
+
+extern "C" int ngs_pcg_block_capacity(int mode) {
+  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64) return 0;
+  return capacity_of(mode);
+}
+
+extern "C" int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode) {
+  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0) return 0;
+  return (int)pcg_blocks_for(n, nnz, 0, capacity_of(mode));
+}
+
+// Validate one system, carve its workspace and fill the kernel arguments (nblocks left 0).
+// Returns NGS_OK, an error, or 1 for an empty system (status written, nothing to launch).
+static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
+                       int64_t* info_dev, double* resid_dev, cudaStream_t st, PcgArgs& a) {
   if (!sys || !cfg || !info_dev || !resid_dev || sys->n < 0 || !sys->rowptr || (sys->nnz > 0 && !sys->cols) ||
       !sys->inv_diag)
     return NGS_ERR_INVALID_ARG;
@@ -578,17 +626,16 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   if (mode == NGS_PCG_MIXED && (!sys->vals32 || !sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
   if (mode == NGS_PCG_FP64 && (!sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
   if (!ws || ws_bytes < ngs_pcg_workspace_bytes(sys->n, mode)) return NGS_ERR_OOM;
-  cudaStream_t st = (cudaStream_t)s;
   const int64_t n = sys->n;
   if (n == 0) {
     cudaMemsetAsync(info_dev, 0, 4 * sizeof(int64_t), st);
     cudaMemsetAsync(resid_dev, 0, 2 * sizeof(double), st);
-    return NGS_OK;
+    return 1;
   }
   const size_t vt = mode == NGS_PCG_REFERENCE ? 4 : 8;
   const size_t rt = mode == NGS_PCG_REFERENCE ? 4 : 8;
   char* base = static_cast<char*>(ws);
-  PcgArgs a{};
+  a = PcgArgs{};
   a.n = n;
   a.nnz = sys->nnz;
   a.rowptr = sys->rowptr;
@@ -611,7 +658,6 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   a.gen = ctl + 1;
   a.error = reinterpret_cast<int*>(ctl + 2);
   a.deadline = reinterpret_cast<unsigned long long*>(ctl + 4);
-  cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned int), st);
   a.info = info_dev;
   a.resid = resid_dev;
   a.tol = cfg->tol;
@@ -621,11 +667,79 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   a.wait_ns = (unsigned long long)(timeout * 1e9);
   a.budget_ns = a.wait_ns;
   a.inner_rtol = 1.0e-4;
-  int rc;
-  if (mode == NGS_PCG_REFERENCE) rc = launch_pcg<NGS_PCG_REFERENCE>(a, cfg->blocks, st);
-  else if (mode == NGS_PCG_MIXED) rc = launch_pcg<NGS_PCG_MIXED>(a, cfg->blocks, st);
-  else rc = launch_pcg<NGS_PCG_FP64>(a, cfg->blocks, st);
-  return rc;
+  return NGS_OK;
+}
+
+static void* pcg_kernel_of(int mode) {
+  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_kernel<NGS_PCG_REFERENCE>;
+  if (mode == NGS_PCG_MIXED) return (void*)pcg_kernel<NGS_PCG_MIXED>;
+  return (void*)pcg_kernel<NGS_PCG_FP64>;
+}
+
+static void* pcg_batch_kernel_of(int mode) {
+  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_batch_kernel<NGS_PCG_REFERENCE>;
+  if (mode == NGS_PCG_MIXED) return (void*)pcg_batch_kernel<NGS_PCG_MIXED>;
+  return (void*)pcg_batch_kernel<NGS_PCG_FP64>;
+}
+
+extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
+                             int64_t* info_dev, double* resid_dev, ngs_stream s) {
+  cudaStream_t st = (cudaStream_t)s;
+  PcgArgs a;
+  const int rc = prepare_pcg(sys, cfg, ws, ws_bytes, info_dev, resid_dev, st, a);
+  if (rc == 1) return NGS_OK;
+  if (rc != NGS_OK) return rc;
+  const int cap = capacity_of(cfg->mode);
+  if (cap < 1) return NGS_ERR_CUDA;
+  const int64_t blocks = pcg_blocks_for(a.n, a.nnz, cfg->blocks, cap);
+  if (blocks < 1) return NGS_ERR_INVALID_ARG;
+  a.nblocks = (unsigned int)blocks;
+  cudaMemsetAsync(a.count, 0, 8 * sizeof(unsigned int), st);
+  void* args[] = {&a};
+  ngs_count_launch();
+  const cudaError_t e = cudaLaunchCooperativeKernel(pcg_kernel_of(cfg->mode), dim3((unsigned)blocks),
+                                                    dim3(PCG_THREADS), args, pcg_smem_bytes(cfg->mode), st);
+  if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  return NGS_OK;
+}
+
+extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items, ngs_stream s) {
+  if (!items || n_items < 0 || n_items > NGS_PCG_BATCH_MAX) return NGS_ERR_INVALID_ARG;
+  if (n_items == 0) return NGS_OK;
+  cudaStream_t st = (cudaStream_t)s;
+  const int mode = items[0].cfg.mode;
+  for (int k = 0; k < n_items; k++)
+    if (items[k].cfg.mode != mode) return NGS_ERR_INVALID_ARG;
+  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64) return NGS_ERR_INVALID_ARG;
+  const int cap = capacity_of(mode);
+  if (cap < 1) return NGS_ERR_CUDA;
+  static thread_local PcgBatch b;          // 15 KB: kept off the stack
+  b.nsys = 0;
+  unsigned int total = 0;
+  // validate and size everything before the first memset, so that a rejected batch touches nothing
+  for (int k = 0; k < n_items; k++) {
+    const ngs_pcg_batch_item& it = items[k];
+    PcgArgs a;
+    const int rc = prepare_pcg(&it.sys, &it.cfg, it.ws, it.ws_bytes, it.info_dev, it.resid_dev, st, a);
+    if (rc == 1) continue;
+    if (rc != NGS_OK) return rc;
+    const int64_t blocks = pcg_blocks_for(a.n, a.nnz, it.cfg.blocks, cap);
+    if (blocks < 1) return NGS_ERR_INVALID_ARG;
+    if (total + blocks > (unsigned)cap) return NGS_ERR_INVALID_ARG;   // not co-resident: split the batch
+    a.nblocks = (unsigned int)blocks;
+    b.start[b.nsys] = total;
+    b.sys[b.nsys++] = a;
+    total += (unsigned)blocks;
+  }
+  if (b.nsys == 0) return NGS_OK;
+  b.start[b.nsys] = total;
+  for (int k = 0; k < b.nsys; k++) cudaMemsetAsync(b.sys[k].count, 0, 8 * sizeof(unsigned int), st);
+  void* args[] = {&b};
+  ngs_count_launch();
+  const cudaError_t e = cudaLaunchCooperativeKernel(pcg_batch_kernel_of(mode), dim3(total), dim3(PCG_THREADS), args,
+                                                    pcg_smem_bytes(mode), st);
+  if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  return NGS_OK;
 }
 
 // ----------------------------------------------------------------------------- solve without allocating

@@ -54,8 +54,12 @@ def reconstruct(xyz, normal, voxel_size: float, depth: int = 4, min_density: flo
     nrm_d, _ = _to_device(normal, dev)
     rec = Reconstruction(xyz_d, nrm_d, voxel_size, depth, min_density, screen_alpha, solver=solver)
     v, f = rec.run(n_upsample)
-    if kind == "cpu":
-        v, f = v.cpu(), f.cpu()
-    elif kind == "numpy":
-        v, f = v.cpu().numpy(), f.cpu().numpy()
+    if kind != "cuda":
+        # pinned host buffers: the copies run at DMA speed instead of through a pageable bounce
+        vh = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+        fh = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+        vh.copy_(v, non_blocking=True)
+        fh.copy_(f, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        v, f = (vh, fh) if kind == "cpu" else (vh.numpy(), fh.numpy())
     return (v, f, rec) if return_reconstruction else (v, f)

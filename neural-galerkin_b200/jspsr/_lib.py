@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import threading
 from pathlib import Path
 
 import numpy as np
@@ -44,6 +45,14 @@ class PcgConfig(C.Structure):
 
 
 G, H = Grid, C.POINTER(HashTable)
+PCG_BATCH_MAX = 64
+
+
+class PcgBatchItem(C.Structure):
+    _fields_ = [("sys", PcgSystem), ("cfg", PcgConfig), ("ws", vp), ("ws_bytes", sz), ("info_dev", vp),
+                ("resid_dev", vp)]
+
+
 _SIGS = {
     "ngs_status_string": ([C.c_int], C.c_char_p),
     "ngs_last_cuda_error": ([], C.c_char_p),
@@ -83,6 +92,9 @@ _SIGS = {
     "ngs_finish_system": ([vp, i64, vp, i64, vp, vp, vp], C.c_int),
     "ngs_pcg_workspace_bytes": ([i64, C.c_int], sz),
     "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
+    "ngs_pcg_block_capacity": ([C.c_int], C.c_int),
+    "ngs_pcg_blocks": ([i64, i64, C.c_int], C.c_int),
+    "ngs_pcg_solve_batch": ([C.POINTER(PcgBatchItem), C.c_int, vp], C.c_int),
     "ngs_pcg_noalloc_max_rows": ([], i64),
     "ngs_pcg_solve_noalloc": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, vp, vp], C.c_int),
     "ngs_spmv64": ([i64, vp, vp, vp, vp, vp, vp], C.c_int),
@@ -160,8 +172,37 @@ def ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_cur_device = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def stream():
+    """The calling thread's current CUDA stream (torch's), as a handle for the C-ABI."""
+    if _raw_stream is not None and _cur_device is not None:
+        return C.c_void_p(_raw_stream(_cur_device()))
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+_dev_tables: dict = {}
+_dev_tables_lock = threading.Lock()
+
+
+def device_table(key, make, device) -> torch.Tensor:
+    """A constant table uploaded once per device: ``make()`` -> numpy / torch host array.  The
+    upload of a pageable host array waits for the stream, so per-call uploads would serialise the
+    host with the GPU."""
+    dev = torch.device(device)
+    k = (key, dev.index)
+    t = _dev_tables.get(k)
+    if t is None:
+        with _dev_tables_lock:
+            t = _dev_tables.get(k)
+            if t is None:
+                a = make()
+                t = (torch.from_numpy(a) if not isinstance(a, torch.Tensor) else a).to(dev)
+                torch.cuda.synchronize(dev)
+                _dev_tables[k] = t
+    return t
 
 
 # ----------------------------------------------------------------------------- helpers

@@ -16,6 +16,7 @@ import torch
 
 from ..bases.hermite_ns import AdditiveHermite
 from ..bases.additive_components import SinPeaks
+from ._hash_backend import compute_density
 from .hashtree import HashTree
 from .reconstructor import Reconstructor
 
@@ -41,9 +42,13 @@ class LearnedStep:
     sample_weight: torch.Tensor = None
 
     def build(self):
-        """Tree and splatting weights (depend on positions only)."""
+        """Tree and splatting weights (depend on positions only).  ``min_density=None`` layers the
+        points at the median of their density (so that no level is empty on any shape)."""
         self.basis = self.basis.to(self.xyz.device)
         self.tree = HashTree(self.xyz, voxel_size=self.voxel_size, depth=self.depth)
+        if self.min_density is None:
+            dens = compute_density(self.xyz, 4 * self.voxel_size) / 16
+            self.min_density = float(torch.median(dens))
         self.tree.build_encoder_hierarchy_adaptive(min_density=self.min_density)
         self.tree.reflect_decoder_coords()
         self.sample_weight = 1.0 / self.tree.xyz_density

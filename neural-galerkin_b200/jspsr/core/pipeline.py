@@ -148,7 +148,7 @@ class Reconstruction:
             raise ValueError("empty point cloud")
         self.vs = float(voxel_size)
         self.depth = int(depth)
-        self.min_density = float(min_density)
+        self.min_density = None if min_density is None else float(min_density)
         self.alpha = float(screen_alpha)
         self.delta = float(screen_delta)
         self.solver = parse_solver(solver)
@@ -159,6 +159,7 @@ class Reconstruction:
         self.solve_stats = {}
         self.profile_pcg = False
         self._pcg_events = {}
+        self.solve_hook = None     # callable(rec, level, d, item): hands the level's PCG to a batcher
 
     def _mark(self, name):
         if self.t is not None:
@@ -187,9 +188,20 @@ class Reconstruction:
         self.density = torch.empty(self.n, dtype=torch.float32, device=self.dev)
         self.point_level = torch.empty(self.n, dtype=torch.int32, device=self.dev)
         self.weight = torch.empty(self.n, dtype=torch.float32, device=self.dev)
+        md = self.min_density if self.min_density is not None else 1.0
         L.call("ngs_density_eval", gd, L.ptr(self.xyz), self.n, np.float32(inv_d), vsd, L.ptr(wd),
-               np.float32(self.min_density), self.depth, L.ptr(self.density), L.ptr(self.point_level),
-               L.ptr(self.weight), st)
+               np.float32(md), self.depth, L.ptr(self.density), L.ptr(self.point_level), L.ptr(self.weight), st)
+        if self.min_density is None:
+            # data-dependent layering (no reference counterpart): the median density, so that the
+            # denser half of the points sits on the finest level and no level is left empty.  It is
+            # rounded down to a quarter power of two: the median itself is a point's density, and the
+            # last bits of a density depend on the order of the splat's atomics, so an unrounded
+            # threshold would put that point on either side from run to run.
+            med = float(torch.median(self.density))
+            md = 2.0 ** (math.floor(4.0 * math.log2(med)) / 4.0) if med > 0 else 1.0
+            L.call("ngs_density_eval", gd, L.ptr(self.xyz), self.n, np.float32(inv_d), vsd, L.ptr(wd),
+                   np.float32(md), self.depth, L.ptr(self.density), L.ptr(self.point_level), L.ptr(self.weight), st)
+        self.min_density_used = md
         self._mark("density")
         # level grids
         q = [np.float32(b[:3]) * np.float32(self.inv_vs), np.float32(b[3:]) * np.float32(self.inv_vs)]
@@ -241,7 +253,7 @@ class Reconstruction:
             lv.cols = torch.empty(lv.nnz, dtype=torch.int32, device=self.dev)
             lv.vals64 = torch.empty(lv.nnz, dtype=torch.float64, device=self.dev)
             lv.diag_slot = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
-            st125 = torch.from_numpy(TB.stencil125(lv.stride)).to(self.dev)
+            st125 = L.device_table(("stencil125", lv.stride), lambda s=lv.stride: TB.stencil125(s), self.dev)
             L.call("ngs_stencil_fill", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(lv.rowptr),
                    L.ptr(st125), L.ptr(lv.cols), L.ptr(lv.vals64), L.ptr(lv.diag_slot), st)
             if self.alpha > 0:
@@ -263,9 +275,10 @@ class Reconstruction:
         for dd, ld in enumerate(self.levels):
             if ld.normals is None:
                 continue
-            tc, tg = TB.rhs_tables(ld.stride, lv.stride)
-            tc = torch.from_numpy(tc).to(self.dev)
-            tg = torch.from_numpy(tg).to(self.dev)
+            tc = L.device_table(("rhs_c", ld.stride, lv.stride), lambda a=ld.stride, b=lv.stride: TB.rhs_tables(a, b)[0],
+                                self.dev)
+            tg = L.device_table(("rhs_g", ld.stride, lv.stride), lambda a=ld.stride, b=lv.stride: TB.rhs_tables(a, b)[1],
+                                self.dev)
             L.call("ngs_rhs_normals", ld.grid, L.ptr(ld.coords), ld.n, L.ptr(ld.normals), lv.grid, L.ptr(lv.coords),
                    lv.n, L.ptr(tc), L.ptr(tg), tc.numel(), L.ptr(rhs), st)
         sf = 0.25 ** d
@@ -283,45 +296,69 @@ class Reconstruction:
                        sf * self.alpha, L.ptr(rhs), st)
             for dd in coarser:
                 lc = self.levels[dd]
-                tc, tg = TB.correction_tables(lv.stride, lc.stride)
-                tc = torch.from_numpy(tc).to(self.dev)
-                tg = torch.from_numpy(tg).to(self.dev)
+                tc = L.device_table(("corr_c", lv.stride, lc.stride),
+                                    lambda a=lv.stride, b=lc.stride: TB.correction_tables(a, b)[0], self.dev)
+                tg = L.device_table(("corr_g", lv.stride, lc.stride),
+                                    lambda a=lv.stride, b=lc.stride: TB.correction_tables(a, b)[1], self.dev)
                 L.call("ngs_correction_stiffness", L.ptr(lv.coords), lv.n, lv.stride, lc.grid, L.ptr(lc.x32),
                        L.ptr(tc), L.ptr(tg), tc.numel(), L.ptr(rhs), st)
         lv.rhs = rhs
         return rhs
 
-    def _solve_level(self, lv: Level, d: int = 0):
+    def pcg_item(self, lv: Level) -> "L.PcgBatchItem":
+        """Output buffers, workspace and the C-ABI description of one level's PCG solve."""
         spec = self.solver
         lv.x32 = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
         lv.x64 = torch.empty(lv.n, dtype=torch.float64, device=self.dev)
         lv.info = torch.zeros(4, dtype=torch.int64, device=self.dev)
         lv.resid = torch.zeros(2, dtype=torch.float64, device=self.dev)
-        if spec.mode is None:
-            return self._solve_plain_fp64(lv)
-        sysd = L.PcgSystem()
+        item = L.PcgBatchItem()
+        sysd = item.sys
         sysd.n, sysd.nnz = lv.n, lv.nnz
         sysd.rowptr, sysd.cols, sysd.inv_diag = lv.rowptr.data_ptr(), lv.cols.data_ptr(), lv.inv_diag.data_ptr()
         sysd.vals32, sysd.vals64 = lv.vals32.data_ptr(), lv.vals64.data_ptr()
         b32 = lv.rhs.float()
         sysd.b32, sysd.b64 = b32.data_ptr(), lv.rhs.data_ptr()
         sysd.x32, sysd.x64 = lv.x32.data_ptr(), lv.x64.data_ptr()
-        cfg = L.PcgConfig()
+        cfg = item.cfg
         cfg.mode, cfg.max_iter, cfg.tol = spec.mode, spec.maxiter, spec.tol
         cfg.res_fix, cfg.replace_every, cfg.blocks, cfg.timeout_s = int(spec.res_fix), spec.replace, 0, spec.timeout
         ws_bytes = L.load().ngs_pcg_workspace_bytes(lv.n, spec.mode)
         ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.dev)
-        if self.profile_pcg:
-            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            ev[0].record()
-        L.call("ngs_pcg_solve", L.C.byref(sysd), L.C.byref(cfg), L.ptr(ws), ws_bytes, L.ptr(lv.info),
-               L.ptr(lv.resid), L.stream())
-        if self.profile_pcg:
-            ev[1].record()
-            self._pcg_events[d] = ev
+        item.ws, item.ws_bytes = ws.data_ptr(), ws_bytes
+        item.info_dev, item.resid_dev = lv.info.data_ptr(), lv.resid.data_ptr()
+        lv._keep = (ws, b32)
+        return item
+
+    def _solve_level(self, lv: Level, d: int = 0):
+        spec = self.solver
+        if spec.mode is None:
+            lv.x32 = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
+            lv.info = torch.zeros(4, dtype=torch.int64, device=self.dev)
+            lv.resid = torch.zeros(2, dtype=torch.float64, device=self.dev)
+            if self.profile_pcg:
+                ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                ev[0].record()
+            self._solve_plain_fp64(lv)
+            if self.profile_pcg:
+                ev[1].record()
+                self._pcg_events[d] = ev
+            return
+        item = self.pcg_item(lv)
+        if self.solve_hook is not None:
+            # batched solve: returns once the solve is enqueued and this stream waits for it
+            self.solve_hook(self, lv, d, item)
+        else:
+            if self.profile_pcg:
+                ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                ev[0].record()
+            L.call("ngs_pcg_solve", L.C.byref(item.sys), L.C.byref(item.cfg), item.ws, item.ws_bytes, item.info_dev,
+                   item.resid_dev, L.stream())
+            if self.profile_pcg:
+                ev[1].record()
+                self._pcg_events[d] = ev
         if spec.mode == L.PCG_REFERENCE:
             lv.x64 = lv.x32.double()
-        lv._keep = (ws, b32)
 
     def _solve_plain_fp64(self, lv: Level):
         """Host-driven FP64 Jacobi-PCG, one launch per vector op and a host check per iteration --
@@ -475,7 +512,7 @@ class Reconstruction:
             lo = np.minimum(lo, n_upsample * (glo - 2 * s))
             hi = np.maximum(hi, n_upsample * (ghi + 3 * s))
         dg, dw = L.make_grid(lo, (hi - lo) + 1, 1, dev)
-        offs = CONFORM_OFFSETS.to(dev)
+        offs = L.device_table("conform_offsets", lambda: CONFORM_OFFSETS, dev)
         for d in range(max_depth):
             L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
                    self.levels[d].stride, st)

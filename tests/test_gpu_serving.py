@@ -1,0 +1,90 @@
+"""Serving path on the GPU: the batched PCG launch against solo solves (bit for bit), and each
+request's result alone against the same request in a concurrent mix."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT / "neural-galerkin_b200"))
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(k, seed=0, n_range=(2000, 60000)):
+    from jspsr import synthetic
+    from jspsr.serving import Request
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(k):
+        req = dict(n=int(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))), seed=1000 + i)
+        x, n = synthetic.serving_request_device(req, "cuda")
+        vs = 2.0 ** -int(rng.integers(6, 9))
+        out.append(Request(x.cpu().pin_memory(), n.cpu().pin_memory(), vs, depth=4, rid=i))
+    return out
+
+
+def test_batched_pcg_is_bit_identical_to_solo_solves():
+    from jspsr import _lib as L
+    from jspsr.core.pipeline import Reconstruction
+    lib = L.load()
+    recs, items, solo = [], [], []
+    for req in _requests(5, seed=1):
+        rec = Reconstruction(req.xyz.cuda(), req.normal.cuda(), req.voxel_size, 4, None, 4.0)
+        rec.build_tree().assemble()
+        d = rec.depth - 1
+        lv = rec.levels[d]
+        rec._rhs(d)
+        item = rec.pcg_item(lv)
+        L.call("ngs_pcg_solve", L.C.byref(item.sys), L.C.byref(item.cfg), item.ws, item.ws_bytes, item.info_dev,
+               item.resid_dev, L.stream())
+        solo.append((lv.x64.clone(), lv.info.clone()))
+        lv.x64.zero_()
+        lv.info.zero_()
+        recs.append(rec)
+        items.append(item)
+    cap = lib.ngs_pcg_block_capacity(items[0].cfg.mode)
+    blocks = [lib.ngs_pcg_blocks(it.sys.n, it.sys.nnz, it.cfg.mode) for it in items]
+    assert sum(blocks) <= cap, (blocks, cap)
+    arr = (L.PcgBatchItem * len(items))(*items)
+    assert lib.ngs_pcg_solve_batch(arr, len(items), L.stream()) == 0
+    torch.cuda.synchronize()
+    for rec, (x, info) in zip(recs, solo):
+        lv = rec.levels[rec.depth - 1]
+        assert int(info[1]) == 0 and int(lv.info[1]) == 0
+        assert torch.equal(lv.info[:3], info[:3])
+        assert torch.equal(lv.x64, x)
+
+
+def test_batched_pcg_rejects_oversubscription():
+    from jspsr import _lib as L
+    lib = L.load()
+    cap = lib.ngs_pcg_block_capacity(L.PCG_MIXED)
+    assert cap >= 148
+    # the capacity query and the solo block count agree with a system sized to need everything
+    assert lib.ngs_pcg_blocks(10_000_000, 1_250_000_000, L.PCG_MIXED) in (0, cap)
+    assert lib.ngs_pcg_blocks(1000, 20000, L.PCG_MIXED) >= 1
+
+
+def test_serving_results_equal_alone_and_mixed():
+    from jspsr.serving import ReconServer, run_sequential
+    reqs = _requests(8, seed=2)
+    alone = run_sequential(reqs, keep_solutions=True)
+    srv = ReconServer(slots=4, keep_solutions=True)
+    try:
+        mixed = srv.run(reqs, realtime=False)
+        launches, systems = srv.batcher.launches, srv.batcher.batched_systems
+    finally:
+        srv.close()
+    assert all(r.error is None for r in mixed), [r.error for r in mixed]
+    assert systems == 8 * 4 and launches < systems      # the solves did share launches
+    for a, m in zip(alone, mixed):
+        for xa, xm in zip(a.solutions, m.solutions):
+            assert float(torch.linalg.norm(xa - xm) / torch.linalg.norm(xa)) <= 1e-6
+        fa, fm = a.faces.numpy(), m.faces.numpy()
+        if fa.shape == fm.shape and np.array_equal(fa, fm):
+            assert np.abs(a.vertices.numpy() - m.vertices.numpy()).max() <= 1e-5
+        else:
+            assert abs(fa.shape[0] - fm.shape[0]) <= max(2, 0.001 * fa.shape[0])
