@@ -24,6 +24,10 @@ LIB = HERE / "jspsr" / "libngs.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-warn-spills", f"-I{INCLUDE}", f"-I{CSRC}"]
+# Per-file flags.  pcg.cu: no multiply-add contraction, so that the single-system and the batched
+# kernel (the same solver body inlined into two kernels) round every operation identically and a
+# batched solve is bit-identical to the solo one; the SpMV is bound by memory, not by the extra adds.
+FILE_FLAGS = {"pcg.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -43,7 +47,7 @@ def compile_one(src: Path, force: bool, verbose_ptxas: bool) -> Path:
     obj = BUILD / (src.stem + ".o")
     if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, _newest_dep()):
         return obj
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if verbose_ptxas:
         cmd[1:1] = ["-Xptxas", "-v"]
     res = subprocess.run(cmd, capture_output=True, text=True)

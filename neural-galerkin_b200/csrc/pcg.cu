@@ -10,6 +10,11 @@
 //     phase B  (own rows)  w = A u, partial dots (r,u), (w,u), (r,r)
 //     barrier + reduce     the last block to arrive sums the per-block partials in
 //                          block order (deterministic) and releases the others.
+// The SpMV streams the CSR arrays straight from HBM: eight lanes per row, each lane
+// with four (column, value) pairs and their vector gathers in flight per round, at
+// two blocks per SM.  (Staging CSR tiles through shared memory with bulk copies ran at
+// less than half this rate: the product and row-sum passes over shared memory, not
+// the copies, bounded it.)
 // Every wait is bounded by the global nanosecond timer; on timeout the kernel
 // records NGS_ERR_TIMEOUT and returns.  Every solve is bounded too: at most
 // NGS_PCG_ITER_CAP iterations, and a deadline that the last block of each
@@ -17,23 +22,25 @@
 // FP64 in every mode.
 //
 // Mixed precision (NGS_PCG_MIXED) is iterative refinement: the inner PCG runs on
-// the FP32 matrix values with FP64 vectors and FP64 accumulation, until its
-// residual has dropped by `inner_rtol`; then the true residual b - A x is formed
-// with the FP64 matrix and the inner solve restarts from it.  The FP32 matrix is
-// a fixed SPD perturbation of the FP64 one, so each outer step contracts the
-// error by about |A32 - A64| |A64^-1| and the solve converges to the FP64 system.
+// the FP32 matrix with FP32 search vectors, FP64 accumulation of every product
+// and dot, and FP64 x and r, until its residual has dropped by `inner_rtol`; then
+// the true residual b - A x is formed with the FP64 matrix and the inner solve
+// restarts from it.  The FP32 matrix is a fixed SPD perturbation of the FP64 one,
+// so each outer step contracts the error by about |A32 - A64| |A64^-1| and the
+// solve converges to the FP64 system.
+//
+// This file is compiled without multiply-add contraction (build.py): the solver body is inlined
+// into the single-system and the batched kernel, and only uncontracted arithmetic is guaranteed to
+// round the same way in both, which makes a batched solve bit-identical to the solo one.
 #include <cmath>
 #include <mutex>
 #include "ngs_common.cuh"
 
 constexpr int PCG_THREADS = 512;
-constexpr int PCG_ROW_LANES = 4;       // lanes per row in the per-row reduction
-constexpr int PCG_TILE_NNZ = 5120;     // non-zeros per shared-memory tile (stage)
-constexpr int PCG_ROW_COST = 8;        // planning cost of a row on top of its non-zeros
-constexpr int PCG_TILE_BODY = PCG_TILE_NNZ - 264;   // cost budget of a tile; whole rows extend it by < 264
-constexpr int PCG_TILE_ROWS = (PCG_TILE_BODY + 264) / (PCG_ROW_COST + 1) + 1;   // rows a tile can hold
-constexpr int PCG_MAX_TILES = 2048;    // tiles a block can own
-constexpr int PCG_STAGES = 2;
+constexpr int PCG_MIN_BLOCKS = 2;      // blocks per SM the register budget is sized for
+constexpr int PCG_ROW_LANES = 8;       // lanes per row in the SpMV
+constexpr int PCG_ROW_COST = 8;        // work of a row on top of its non-zeros (vector traffic)
+constexpr int PCG_BLOCK_WORK = 16384;  // work (non-zeros + row cost) that justifies one more block
 
 struct PcgArgs {
   int64_t n;
@@ -79,43 +86,6 @@ NGS_DEV unsigned long long global_ns() {
 template <typename T>
 NGS_DEV T ld_cg(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
 
-// ----------------------------------------------------------------------------- bulk copies (no multicast)
-NGS_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-NGS_DEV void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-NGS_DEV void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-NGS_DEV void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-NGS_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-NGS_DEV bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  uint32_t ok;
-  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-               : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-  return ok != 0;
-}
-
-// Per-block state of the tiled SpMV: rows [row0, row1) owned by the block, split into tiles of
-// whole rows of at most PCG_TILE_NNZ non-zeros; tile t covers rows [tiles[t], tiles[t+1]).
-struct BlockRows {
-  int64_t row0, row1, ebase;
-  int ntiles;
-  int32_t* tiles;              // shared: first row of tile t (block-relative), [ntiles + 1]
-  int32_t* tile_e;             // shared: first non-zero of tile t (relative to ebase), [ntiles + 1]
-  int32_t* srp;                // shared: row offsets of the current tile, [PCG_TILE_ROWS + 1]
-  double2* aux;                // shared: epilogue operands of the current tile's rows, [PCG_TILE_ROWS]
-  double* prod;                // shared: products of the current tile, [PCG_TILE_NNZ]
-  unsigned long long* bars;    // shared, one mbarrier per stage
-  char* stage;                 // shared, PCG_STAGES stages
-  size_t stage_bytes;
-  unsigned phase;              // parity bits, one per stage (block-uniform)
-};
-
 // Block b owns the rows whose first non-zero lies in [b * nnz / B, (b + 1) * nnz / B).
 NGS_DEV int64_t first_row_at(const int64_t* __restrict__ rp, int64_t n, int64_t e) {
   int64_t lo = 0, hi = n;
@@ -126,140 +96,60 @@ NGS_DEV int64_t first_row_at(const int64_t* __restrict__ rp, int64_t n, int64_t 
   return lo;
 }
 
-// Tile starts: a row costs its non-zeros plus PCG_ROW_COST; tile k holds the rows whose last cost unit
-// falls in [k, k+1) * PCG_TILE_BODY (block-relative), so a tile holds at most PCG_TILE_NNZ non-zeros and
-// PCG_TILE_ROWS rows.  Rows longer than PCG_MAX_ROW, or empty, are rejected.  Returns false for such a block.
-constexpr int PCG_MAX_ROW = 250;
-
-NGS_DEV bool plan_tiles(const PcgArgs& a, unsigned bid, BlockRows& br) {
+// Rows [row0, row1) of block bid, and whether every one of them holds at least one entry
+// (an SPD row holds its diagonal); the check is block-uniform.
+NGS_DEV bool block_rows(const PcgArgs& a, unsigned bid, int64_t& row0, int64_t& row1) {
   __shared__ int64_t bounds[2];
-  __shared__ int nt, bad;
+  __shared__ int bad;
   if (threadIdx.x == 0) {
     const int64_t B = a.nblocks;
     bounds[0] = first_row_at(a.rowptr, a.n, (a.nnz * (int64_t)bid) / B);
     bounds[1] = bid + 1 == a.nblocks ? a.n : first_row_at(a.rowptr, a.n, (a.nnz * ((int64_t)bid + 1)) / B);
-    nt = 0;
     bad = 0;
   }
   __syncthreads();
-  br.row0 = bounds[0];
-  br.row1 = bounds[1];
-  const int64_t base = br.row0 < br.row1 ? a.rowptr[br.row0] : 0;
-  for (int64_t r = br.row0 + threadIdx.x; r < br.row1; r += blockDim.x) {
-    const int64_t e0 = a.rowptr[r], e1 = a.rowptr[r + 1];
-    if (e1 - e0 > PCG_MAX_ROW || e1 <= e0) bad = 1;   // SPD rows hold at least their diagonal
-    // index of the tile holding the row's last cost unit
-    const int64_t d1 = (e1 - base) + (int64_t)PCG_ROW_COST * (r + 1 - br.row0);
-    const int64_t d0 = (e0 - base) + (int64_t)PCG_ROW_COST * (r - br.row0);
-    const int64_t k = (d1 + PCG_TILE_BODY - 1) / PCG_TILE_BODY - 1;
-    const int64_t kp = r == br.row0 ? -1 : (d0 + PCG_TILE_BODY - 1) / PCG_TILE_BODY - 1;
-    for (int64_t t = kp + 1; t <= k && t < PCG_MAX_TILES; t++) br.tiles[t] = (int32_t)(r - br.row0);
-    if (r + 1 == br.row1) nt = (int)(k + 1 < PCG_MAX_TILES ? k + 1 : PCG_MAX_TILES);
-  }
-  __syncthreads();
-  br.ntiles = br.row0 < br.row1 ? (nt > 0 ? nt : 1) : 0;
-  br.ebase = base;
-  if (threadIdx.x == 0 && br.ntiles > 0) {
-    br.tiles[0] = 0;
-    br.tiles[br.ntiles] = (int32_t)(br.row1 - br.row0);
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t <= br.ntiles; t += blockDim.x) br.tile_e[t] = (int32_t)(a.rowptr[br.row0 + br.tiles[t]] - base);
-  __syncthreads();
-  return bad == 0;
+  row0 = bounds[0];
+  row1 = bounds[1];
+  for (int64_t r = row0 + threadIdx.x; r < row1; r += blockDim.x)
+    if (a.rowptr[r + 1] <= a.rowptr[r]) bad = 1;
+  return __syncthreads_or(bad) == 0;
 }
 
-// Issue the bulk copies of tile t into stage st: the 16-byte aligned body of its column and value
-// ranges; the ragged tail (< 4 elements) is read from global memory by the consumer.
-template <typename MT>
-NGS_DEV void issue_tile(const PcgArgs& a, const MT* vals, BlockRows& br, int t, int st) {
-  if (threadIdx.x != 0) return;
-  const int64_t e0 = br.ebase + br.tile_e[t], e1 = br.ebase + br.tile_e[t + 1];
-  constexpr int64_t VA = 16 / sizeof(MT);
-  const int64_t c0 = e0 & ~3ll, c1 = e1 & ~3ll, v0 = e0 & ~(VA - 1), v1 = e1 & ~(VA - 1);
-  const unsigned cb = (unsigned)((c1 > c0 ? c1 - c0 : 0) * 4), vb = (unsigned)((v1 > v0 ? v1 - v0 : 0) * sizeof(MT));
-  char* dst = br.stage + st * br.stage_bytes;
-  mbar_expect_tx(&br.bars[st], cb + vb);
-  if (cb) bulk_g2s(dst, a.cols + c0, cb, &br.bars[st]);
-  if (vb) bulk_g2s(dst + PCG_TILE_NNZ * 4, vals + v0, vb, &br.bars[st]);
-}
+// Streaming loads of the (immutable) matrix: read-only path, no L1 allocation.
+template <typename T>
+NGS_DEV T ld_stream(const T* p) { return __ldg(p); }
 
-// y = A v over the block's rows; epi(row, acc) consumes each row's product and returns a
-// contribution to the block's partial sum.  Returns false if a copy wait timed out.
+// y = A v over rows [row0, row1): eight lanes per row.  epi(row, acc, pre(row)) consumes each
+// row's product (lane 0 of its group) and returns a contribution to the thread's partial sum.
+// The gathered vector is read with plain loads: it was written earlier in this launch.  Ends with a
+// block barrier, after which every thread may read the rows written by the epilogue.
 template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
-NGS_DEV bool spmv_tiles(const PcgArgs& a, const MT* __restrict__ vals, const VT* __restrict__ v, BlockRows& br,
-                        Pre pre, Epi epi, double& dsum) {
-  const int lane = threadIdx.x & (PCG_ROW_LANES - 1);
-  const int group = threadIdx.x / PCG_ROW_LANES, ngroups = PCG_THREADS / PCG_ROW_LANES;
-  const unsigned gmask = ((1u << PCG_ROW_LANES) - 1u) << ((threadIdx.x & 31) & ~(PCG_ROW_LANES - 1));
-  constexpr int64_t VA = 16 / sizeof(MT);
-  for (int t = 0; t < PCG_STAGES && t < br.ntiles; t++) issue_tile(a, vals, br, t, t);
-  bool ok = true;
-  for (int t = 0; t < br.ntiles; t++) {
-    const int st = t % PCG_STAGES;
-    const unsigned par = (br.phase >> st) & 1u;
-    int mine = 1;
-    if (ok) {
-      const unsigned long long t0 = global_ns();
-      while (!mbar_try_wait(&br.bars[st], par)) {
-        if (global_ns() - t0 > a.wait_ns) {
-          atomicExch(a.error, NGS_ERR_TIMEOUT);
-          mine = 0;
-          break;
-        }
-      }
+NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
+                       Pre pre, Epi epi, double& dsum) {
+  constexpr int L = PCG_ROW_LANES;
+  const int sub = threadIdx.x & (L - 1);
+  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+  const int64_t step = blockDim.x / L;
+  for (int64_t row = row0 + threadIdx.x / L; row < row1; row += step) {
+    const int64_t e0 = a.rowptr[row], e1 = a.rowptr[row + 1];
+    const double2 ax = pre(row);
+    ACC acc = (ACC)0;
+    int64_t j = e0 + sub;
+    for (; j + 3 * L < e1; j += 4 * L) {
+      const int32_t c0 = ld_stream(a.cols + j), c1 = ld_stream(a.cols + j + L);
+      const int32_t c2 = ld_stream(a.cols + j + 2 * L), c3 = ld_stream(a.cols + j + 3 * L);
+      const MT m0 = ld_stream(vals + j), m1 = ld_stream(vals + j + L);
+      const MT m2 = ld_stream(vals + j + 2 * L), m3 = ld_stream(vals + j + 3 * L);
+      const VT x0 = v[c0], x1 = v[c1], x2 = v[c2], x3 = v[c3];
+      acc += (ACC)m0 * (ACC)x0 + (ACC)m1 * (ACC)x1 + (ACC)m2 * (ACC)x2 + (ACC)m3 * (ACC)x3;
     }
-    ok = __syncthreads_and(ok && mine) != 0;   // block-uniform outcome of the wait
-    br.phase ^= 1u << st;
-    if (!ok) continue;             // a copy wait gave up: issue nothing more, consume nothing
-    const char* sm = br.stage + st * br.stage_bytes;
-    const int32_t* scol = reinterpret_cast<const int32_t*>(sm);
-    const MT* sval = reinterpret_cast<const MT*>(sm + PCG_TILE_NNZ * 4);
-    const int64_t r_lo = br.row0 + br.tiles[t], r_hi = br.row0 + br.tiles[t + 1];
-    const int64_t e0 = br.ebase + br.tile_e[t], e1 = br.ebase + br.tile_e[t + 1];
-    const int64_t c0 = e0 & ~3ll, c1 = e1 & ~3ll, v0 = e0 & ~(VA - 1), v1 = e1 & ~(VA - 1);
-    ACC* prod = reinterpret_cast<ACC*>(br.prod);
-    // pass 1: every product of the tile.  Fully unrolled and predicated, so that each thread has
-    // all of its gathers in flight at once; the tile's row offsets are staged alongside.
-    constexpr int PER = (PCG_TILE_NNZ + PCG_THREADS - 1) / PCG_THREADS;
-    int32_t cc[PER];
-    MT mm[PER];
+    for (; j < e1; j += L) acc += (ACC)ld_stream(vals + j) * (ACC)v[ld_stream(a.cols + j)];
 #pragma unroll
-    for (int k = 0; k < PER; k++) {
-      const int64_t j = e0 + threadIdx.x + (int64_t)k * PCG_THREADS;
-      cc[k] = -1;
-      mm[k] = (MT)0;
-      if (j < e1) {
-        cc[k] = j < c1 ? scol[j - c0] : __ldg(a.cols + j);
-        mm[k] = j < v1 ? sval[j - v0] : __ldg(vals + j);
-      }
-    }
-    VT vv[PER];
-#pragma unroll
-    for (int k = 0; k < PER; k++) vv[k] = cc[k] >= 0 ? v[cc[k]] : (VT)0;
-    for (int64_t rr = r_lo + threadIdx.x; rr <= r_hi; rr += PCG_THREADS) {
-      br.srp[rr - r_lo] = (int32_t)(a.rowptr[rr] - e0);
-      if (rr < r_hi) br.aux[rr - r_lo] = pre(rr);
-    }
-#pragma unroll
-    for (int k = 0; k < PER; k++) {
-      const int64_t j = e0 + threadIdx.x + (int64_t)k * PCG_THREADS;
-      if (j < e1) prod[j - e0] = (ACC)mm[k] * (ACC)vv[k];
-    }
-    __syncthreads();
-    // pass 2: per-row sums from shared memory
-    for (int64_t row = r_lo + group; row < r_hi; row += ngroups) {
-      const int beg = br.srp[row - r_lo], end = br.srp[row - r_lo + 1];
-      ACC acc = (ACC)0;
-      for (int k = beg + lane; k < end; k += PCG_ROW_LANES) acc += prod[k];
-#pragma unroll
-      for (int o = PCG_ROW_LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
-      if (lane == 0) dsum += epi(row, (double)acc, br.aux[row - r_lo]);
-    }
-    __syncthreads();
-    if (t + PCG_STAGES < br.ntiles) issue_tile(a, vals, br, t + PCG_STAGES, st);
+    for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
+    if (sub == 0) dsum += epi(row, (double)acc, ax);
   }
-  return ok;
+  // the epilogue wrote rows that other threads of the block read next (their rows in phase A)
+  __syncthreads();
 }
 
 // Block sums of NV doubles -> per-block partials -> fixed-order grid reduction.
@@ -342,15 +232,8 @@ NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0
 template <int MODE>
 struct PcgTypes;
 template <> struct PcgTypes<NGS_PCG_REFERENCE> { using MT = float; using VT = float; using RT = float; using ACC = float; };
-template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = double; using RT = double; using ACC = double; };
+template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = float; using RT = double; using ACC = double; };
 template <> struct PcgTypes<NGS_PCG_FP64> { using MT = double; using VT = double; using RT = double; using ACC = double; };
-
-// Bytes of dynamic shared memory the kernel of a mode needs (tile stages + tile plan + mbarriers).
-constexpr size_t pcg_stage_bytes(int mode) { return (size_t)PCG_TILE_NNZ * (4 + (mode == NGS_PCG_REFERENCE ? 4 : 8)); }
-constexpr size_t pcg_smem_bytes(int mode) {
-  return (size_t)PCG_STAGES * pcg_stage_bytes(mode) + (size_t)PCG_TILE_NNZ * 8 + (size_t)PCG_TILE_ROWS * 16 +
-         ((PCG_TILE_ROWS + 4) * 4 + 15) / 16 * 16 + 2 * (PCG_MAX_TILES + 4) * 4 + 64;
-}
 
 // The solve of one system by the blocks bid = 0 .. a.nblocks-1 of a launch (all of them for a
 // single solve, a contiguous range for one system of a batch).
@@ -360,7 +243,6 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
   using VT = typename PcgTypes<MODE>::VT;
   using RT = typename PcgTypes<MODE>::RT;
   using ACC = typename PcgTypes<MODE>::ACC;
-  extern __shared__ __align__(128) char smem[];
   const RT* b = static_cast<const RT*>(a.b);
   RT* x = static_cast<RT*>(a.x);
   RT* r = static_cast<RT*>(a.r);
@@ -371,40 +253,17 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
   const MT* vals = static_cast<const MT*>(a.vals);
   const int sqrt_n = (int)ceil(sqrt((double)a.n));
 
-  // shared layout: [stages][cols | vals] , tile plan, mbarriers
-  constexpr size_t stage_bytes = pcg_stage_bytes(MODE);
-  BlockRows br;
-  char* sp = smem;
-  br.stage = sp;
-  br.stage_bytes = stage_bytes;
-  sp += PCG_STAGES * stage_bytes;
-  br.prod = reinterpret_cast<double*>(sp);
-  sp += (size_t)PCG_TILE_NNZ * 8;
-  br.aux = reinterpret_cast<double2*>(sp);
-  sp += (size_t)PCG_TILE_ROWS * 16;
-  br.srp = reinterpret_cast<int32_t*>(sp);
-  sp += ((size_t)(PCG_TILE_ROWS + 4) * 4 + 15) / 16 * 16;
-  br.tiles = reinterpret_cast<int32_t*>(sp);
-  sp += (size_t)(PCG_MAX_TILES + 4) * 4;
-  br.tile_e = reinterpret_cast<int32_t*>(sp);
-  sp += (size_t)(PCG_MAX_TILES + 4) * 4;
-  br.bars = reinterpret_cast<unsigned long long*>(sp);
-  br.phase = 0;
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < PCG_STAGES; i++) mbar_init(&br.bars[i], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  const bool rows_ok = plan_tiles(a, bid, br);
-  const int64_t i0 = br.row0 + threadIdx.x, i1 = br.row1, is = PCG_THREADS;
+  int64_t row0, row1;
+  const bool rows_ok = block_rows(a, bid, row0, row1);
+  const int64_t i0 = row0 + threadIdx.x, i1 = row1, is = PCG_THREADS;
 
-  // w = A u; returns (w, u).  The row's u is prefetched during the tile's product pass.
+  // w = A u; returns (w, u).
   auto w_pre = [&](int64_t row) -> double2 { return make_double2((double)u[row], 0.0); };
   auto w_epi = [&](int64_t row, double acc, double2 ax) -> double {
     w[row] = (VT)acc;
     return acc * ax.x;
   };
-  // r = b - A x, u = M r; returns (r, r).  b and 1/diag of the row are prefetched.
+  // r = b - A x, u = M r; returns (r, r).
   auto res_pre = [&](int64_t row) -> double2 { return make_double2((double)b[row], (double)a.inv_diag[row]); };
   auto true_res_epi = [&](int64_t row, double acc, double2 ax) -> double {
     const RT ri = (RT)(ax.x - acc);
@@ -412,14 +271,14 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
     u[row] = (VT)(ax.y * (double)ri);
     return (double)ri * (double)ri;
   };
-  // The FP64 true-residual SpMV of MIXED mode streams the FP64 values through the same stages
-  // (the stage holds PCG_TILE_NNZ doubles in MIXED mode); REFERENCE mode replaces with the FP32 matrix.
-  auto spmv_true = [&](double& sum) -> bool {
-    if constexpr (MODE == NGS_PCG_MIXED) return spmv_tiles<double, RT, double>(a, a.vals64, x, br, res_pre, true_res_epi, sum);
-    else return spmv_tiles<MT, RT, ACC>(a, vals, x, br, res_pre, true_res_epi, sum);
+  // the true residual uses the FP64 matrix in MIXED mode, the recurrence matrix otherwise
+  auto spmv_true = [&](double& sum) {
+    if constexpr (MODE == NGS_PCG_MIXED) spmv_rows<double, RT, double>(a, a.vals64, x, row0, row1, res_pre, true_res_epi, sum);
+    else spmv_rows<MT, RT, ACC>(a, vals, x, row0, row1, res_pre, true_res_epi, sum);
   };
+  auto spmv_w = [&](double& sum) { spmv_rows<MT, VT, ACC>(a, vals, u, row0, row1, w_pre, w_epi, sum); };
 
-  // init: x = 0, r = b, u = M r, p = s = 0; partial (b, b); part[1] flags rows too long for a tile
+  // init: x = 0, r = b, u = M r, p = s = 0; partial (b, b); part[1] flags empty rows
   double part[3] = {0.0, rows_ok ? 0.0 : 1.0, 0.0}, res[3];
   for (int64_t i = i0; i < i1; i += is) {
     const RT bi = b[i];
@@ -441,7 +300,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
   const double bnorm = sqrt(res[0]);
   const double atol = a.tol * bnorm;
   part[0] = part[1] = part[2] = 0.0;
-  if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
+  spmv_w(part[1]);
   for (int64_t i = i0; i < i1; i += is) {
     part[0] += (double)r[i] * (double)u[i];
     part[2] += (double)r[i] * (double)r[i];
@@ -481,14 +340,14 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
       // residual replacement: r = b - A x (FP64 matrix in MIXED mode, the FP32 one in REFERENCE mode)
       if (!plain_barrier(a, bid)) return;
       double rr = 0.0;
-      if (!spmv_true(rr)) return;
+      spmv_true(rr);
       part[2] = rr;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       replacements++;
     }
     if (!plain_barrier(a, bid)) return;
     // phase B: w = A u and (w, u)
-    if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
+    spmv_w(part[1]);
     if (!reduce_barrier<3>(a, bid, part, res)) return;
     it++;
     const double gamma_new = res[0];
@@ -499,11 +358,11 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
       // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
       if (!plain_barrier(a, bid)) return;
       part[0] = part[1] = part[2] = 0.0;
-      if (!spmv_true(part[2])) return;
+      spmv_true(part[2]);
       replacements++;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       if (!plain_barrier(a, bid)) return;
-      if (!spmv_tiles<MT, VT, ACC>(a, vals, u, br, w_pre, w_epi, part[1])) return;
+      spmv_w(part[1]);
       if (!reduce_barrier<3>(a, bid, part, res)) return;
       rho = res[2];
       if (sqrt(rho) <= atol) { converged = true; break; }
@@ -531,7 +390,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(PCG_THREADS, 1) pcg_kernel(const __grid_constant__ PcgArgs a) {
+__global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_kernel(const __grid_constant__ PcgArgs a) {
   pcg_body<MODE>(a, blockIdx.x);
 }
 
@@ -547,7 +406,7 @@ struct PcgBatch {
 static_assert(sizeof(PcgBatch) <= 32000, "batch arguments must fit the kernel parameter space");
 
 template <int MODE>
-__global__ void __launch_bounds__(PCG_THREADS, 1) pcg_batch_kernel(const __grid_constant__ PcgBatch b) {
+__global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_batch_kernel(const __grid_constant__ PcgBatch b) {
   int lo = 0, hi = b.nsys - 1;              // last system whose first block is <= blockIdx.x
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -558,43 +417,42 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) pcg_batch_kernel(const __grid_
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Element sizes of a mode's workspace vectors: search vectors (p, s, u, w) and residual r.  The one
+// definition that both the size query and the carve-up use.
+static size_t pcg_vec_bytes(int mode) { return mode == NGS_PCG_FP64 ? 8 : 4; }
+static size_t pcg_res_bytes(int mode) { return mode == NGS_PCG_REFERENCE ? 4 : 8; }
+
 extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
-  const size_t vt = mode == NGS_PCG_REFERENCE ? 4 : 8;
-  const size_t rt = mode == NGS_PCG_REFERENCE ? 4 : 8;
+  const size_t vt = pcg_vec_bytes(mode);
+  const size_t rt = pcg_res_bytes(mode);
   size_t bytes = align_up(n * rt) + 4 * align_up(n * vt);     // r, p, s, u, w
   bytes += align_up((size_t)148 * 32 * 4 * sizeof(double));    // partials (upper bound of blocks)
   bytes += align_up(4 * sizeof(double)) + align_up(8 * sizeof(unsigned int));
   return bytes;
 }
 
-// Blocks one solve uses: as many co-resident blocks as fit, fewer for small systems (about one
-// tile of work each); 0 if the system is too large for the tile plan.
+// Co-resident blocks of the cooperative kernel on the current device.
 template <int MODE>
 static int pcg_capacity() {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = pcg_smem_bytes(MODE);
-  if (cudaFuncSetAttribute(pcg_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaFuncSetAttribute(pcg_batch_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-          cudaSuccess)
-    return 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, 0);
+  int per_sm_batch = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_batch, pcg_batch_kernel<MODE>, PCG_THREADS, 0);
+  if (per_sm_batch < per_sm) per_sm = per_sm_batch;
   const int64_t cap = (int64_t)sms * per_sm;
   return (int)(cap < 148 * 32 ? cap : 148 * 32);
 }
 
+// Blocks one solve uses: as many co-resident blocks as fit, fewer for small systems (about
+// PCG_BLOCK_WORK non-zeros each, so that an iteration's critical path stays short).
 static int64_t pcg_blocks_for(int64_t n, int64_t nnz, int blocks_req, int capacity) {
   int64_t blocks = capacity;
-  // one tile of work per block when the system is small: the iteration's critical path is then one
-  // staged tile plus the two grid barriers
-  const int64_t need = (nnz + (int64_t)PCG_ROW_COST * n + PCG_TILE_BODY - 1) / PCG_TILE_BODY;
+  const int64_t need = (nnz + (int64_t)PCG_ROW_COST * n + PCG_BLOCK_WORK - 1) / PCG_BLOCK_WORK;
   if (blocks > need) blocks = need > 0 ? need : 1;
   if (blocks_req > 0 && blocks_req < blocks) blocks = blocks_req;
-  if (blocks < 1) return 0;
-  // a block owns at most PCG_MAX_TILES tiles
-  if ((nnz + (int64_t)PCG_ROW_COST * n) / blocks + 512 > (int64_t)(PCG_MAX_TILES - 2) * PCG_TILE_BODY) return 0;
-  return blocks;
+  return blocks < 1 ? 0 : blocks;
 }
 
 static int capacity_of(int mode) {
@@ -632,8 +490,8 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
     cudaMemsetAsync(resid_dev, 0, 2 * sizeof(double), st);
     return 1;
   }
-  const size_t vt = mode == NGS_PCG_REFERENCE ? 4 : 8;
-  const size_t rt = mode == NGS_PCG_REFERENCE ? 4 : 8;
+  const size_t vt = pcg_vec_bytes(mode);
+  const size_t rt = pcg_res_bytes(mode);
   char* base = static_cast<char*>(ws);
   a = PcgArgs{};
   a.n = n;
@@ -698,7 +556,7 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   void* args[] = {&a};
   ngs_count_launch();
   const cudaError_t e = cudaLaunchCooperativeKernel(pcg_kernel_of(cfg->mode), dim3((unsigned)blocks),
-                                                    dim3(PCG_THREADS), args, pcg_smem_bytes(cfg->mode), st);
+                                                    dim3(PCG_THREADS), args, 0, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }
@@ -737,7 +595,7 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
   void* args[] = {&b};
   ngs_count_launch();
   const cudaError_t e = cudaLaunchCooperativeKernel(pcg_batch_kernel_of(mode), dim3(total), dim3(PCG_THREADS), args,
-                                                    pcg_smem_bytes(mode), st);
+                                                    0, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }

@@ -18,7 +18,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libngs.so"
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "buffer or workspace too small", 3: "hash insert failed",
           4: "not converged", 5: "topology error", 6: "CUDA error", 7: "device-side wait timed out"}
-NGS_OK, NGS_ERR_NOT_CONVERGED, NGS_ERR_TIMEOUT = 0, 4, 7
+NGS_OK, NGS_ERR_INVALID_ARG, NGS_ERR_NOT_CONVERGED, NGS_ERR_TIMEOUT = 0, 1, 4, 7
 PCG_REFERENCE, PCG_MIXED, PCG_FP64 = 0, 1, 2
 
 vp, i32, i64, f32, f64, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_double, C.c_size_t

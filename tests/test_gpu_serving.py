@@ -31,7 +31,7 @@ def test_batched_pcg_is_bit_identical_to_solo_solves():
     from jspsr.core.pipeline import Reconstruction
     lib = L.load()
     recs, items, solo = [], [], []
-    for req in _requests(5, seed=1):
+    for req in _requests(6, seed=1, n_range=(1500, 20000)):
         rec = Reconstruction(req.xyz.cuda(), req.normal.cuda(), req.voxel_size, 4, None, 4.0)
         rec.build_tree().assemble()
         d = rec.depth - 1
@@ -46,8 +46,17 @@ def test_batched_pcg_is_bit_identical_to_solo_solves():
         recs.append(rec)
         items.append(item)
     cap = lib.ngs_pcg_block_capacity(items[0].cfg.mode)
-    blocks = [lib.ngs_pcg_blocks(it.sys.n, it.sys.nnz, it.cfg.mode) for it in items]
-    assert sum(blocks) <= cap, (blocks, cap)
+    # the largest prefix-greedy subset whose blocks fit one cooperative launch
+    keep, used = [], 0
+    for k, it in enumerate(items):
+        b = lib.ngs_pcg_blocks(it.sys.n, it.sys.nnz, it.cfg.mode)
+        if used + b <= cap:
+            keep.append(k)
+            used += b
+    assert len(keep) >= 2, "need at least two systems in the batch"
+    recs = [recs[k] for k in keep]
+    solo = [solo[k] for k in keep]
+    items = [items[k] for k in keep]
     arr = (L.PcgBatchItem * len(items))(*items)
     assert lib.ngs_pcg_solve_batch(arr, len(items), L.stream()) == 0
     torch.cuda.synchronize()
@@ -59,13 +68,29 @@ def test_batched_pcg_is_bit_identical_to_solo_solves():
 
 
 def test_batched_pcg_rejects_oversubscription():
+    """A batch whose blocks exceed one cooperative launch is refused before anything runs."""
     from jspsr import _lib as L
+    from jspsr.core.pipeline import Reconstruction
     lib = L.load()
     cap = lib.ngs_pcg_block_capacity(L.PCG_MIXED)
     assert cap >= 148
-    # the capacity query and the solo block count agree with a system sized to need everything
-    assert lib.ngs_pcg_blocks(10_000_000, 1_250_000_000, L.PCG_MIXED) in (0, cap)
-    assert lib.ngs_pcg_blocks(1000, 20000, L.PCG_MIXED) >= 1
+    req = _requests(1, seed=3, n_range=(60000, 60001))[0]
+    rec = Reconstruction(req.xyz.cuda(), req.normal.cuda(), 1 / 512, 4, None, 4.0)
+    rec.build_tree().assemble()
+    for d in range(rec.depth - 1, 0, -1):
+        rec._rhs(d)
+        rec._solve_level(rec.levels[d], d)
+    rec._rhs(0)
+    item = rec.pcg_item(rec.levels[0])
+    b = lib.ngs_pcg_blocks(item.sys.n, item.sys.nnz, item.cfg.mode)
+    copies = cap // b + 1
+    if copies > L.PCG_BATCH_MAX:
+        pytest.skip("system too small to oversubscribe within the batch limit")
+    arr = (L.PcgBatchItem * copies)(*([item] * copies))
+    info0 = rec.levels[0].info.clone()
+    assert lib.ngs_pcg_solve_batch(arr, copies, L.stream()) == L.NGS_ERR_INVALID_ARG
+    torch.cuda.synchronize()
+    assert torch.equal(rec.levels[0].info, info0)          # nothing was launched or cleared
 
 
 def test_serving_results_equal_alone_and_mixed():
