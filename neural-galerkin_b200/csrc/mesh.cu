@@ -1,5 +1,6 @@
 // Multi-level dual marching cubes (jspsr/core/reconstructor.py:296-397,
 // csrc/marching_cubes/dual_mc_inds.cu:45-182, dual_mc.cu:20-189).
+#include <algorithm>
 #include "ngs_common.cuh"
 #include "hash_table.cuh"
 
@@ -298,29 +299,91 @@ __global__ void vd_sort_kernel(const int64_t* __restrict__ start, const int32_t*
   const int lane = threadIdx.x & 31;
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t b = warp0; b < nb; b += nwarps) {
-    const int c = count[b];
-    if (c <= 1) {
-      if (c == 1 && lane == 0) first[start[b]] = 1;
-      continue;
+  // a warp reads 32 bucket counts at once (most buckets are empty or hold one key), then sorts the
+  // buckets of 2..512 keys among them one after the other
+  for (int64_t base = warp0 * 32; base < nb; base += nwarps * 32) {
+    const int64_t b = base + lane;
+    const int c = b < nb ? count[b] : 0;
+    if (c == 1) first[start[b]] = 1;
+    unsigned todo = __ballot_sync(0xffffffffu, c >= 2 && c <= 512);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int cb = __shfl_sync(0xffffffffu, c, src);
+      const int64_t s0 = start[base + src];
+      if (cb <= 32) vd_rank_sort<1>(s0, cb, lane, sorted, first);
+      else if (cb <= 128) vd_rank_sort<4>(s0, cb, lane, sorted, first);
+      else vd_rank_sort<16>(s0, cb, lane, sorted, first);
     }
-    const int64_t s0 = start[b];
-    if (c <= 32) vd_rank_sort<1>(s0, c, lane, sorted, first);
-    else if (c <= 128) vd_rank_sort<4>(s0, c, lane, sorted, first);
-    else if (c <= 512) vd_rank_sort<16>(s0, c, lane, sorted, first);
-    else if (lane == 0) {
-      // bucket beyond 512 keys (not produced by the dual grids here): serial insertion sort
-      for (int i = 1; i < c; i++) {
-        const int64_t key = sorted[s0 + i];
-        int j = i - 1;
-        while (j >= 0 && sorted[s0 + j] > key) {
-          sorted[s0 + j + 1] = sorted[s0 + j];
-          j--;
+    // larger buckets (the corners of coarse cells shared by many fine dual cubes): vd_sort_big_kernel
+  }
+}
+
+// Buckets of more than 512 keys: one block per bucket, bitonic sort in shared memory (up to
+// VD_BIG_MAX keys); beyond that one thread sorts by insertion (not produced by these dual grids).
+// Each block scans a contiguous stretch of the bucket counts, 256 at a time, collects the large
+// ones and sorts them one after the other.
+constexpr int VD_BIG_MAX = 4096;
+
+__global__ void __launch_bounds__(256) vd_sort_big_kernel(const int64_t* __restrict__ start,
+                                                          const int32_t* __restrict__ count, int64_t nb,
+                                                          int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
+  __shared__ int64_t keys[VD_BIG_MAX];
+  __shared__ int64_t found[256];
+  __shared__ int nfound;
+  const int64_t per = (nb + gridDim.x - 1) / gridDim.x;
+  const int64_t b0 = (int64_t)blockIdx.x * per, b1 = min(nb, b0 + per);
+  for (int64_t base = b0; base < b1; base += blockDim.x) {
+    if (threadIdx.x == 0) nfound = 0;
+    __syncthreads();
+    const int64_t b = base + threadIdx.x;
+    if (b < b1 && count[b] > 512) found[atomicAdd(&nfound, 1)] = b;
+    __syncthreads();
+    const int nf = nfound;
+    for (int f = 0; f < nf; f++) {
+      const int64_t bk = found[f];
+      const int64_t s0 = start[bk];
+      const int c = count[bk];
+      if (c <= VD_BIG_MAX) {
+        int P = 1;
+        while (P < c) P <<= 1;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) keys[i] = i < c ? sorted[s0 + i] : INT64_MAX;
+        __syncthreads();
+        for (int k = 2; k <= P; k <<= 1) {
+          for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+              const int l = i ^ j;
+              if (l > i) {
+                const int64_t a = keys[i], bb = keys[l];
+                const bool up = (i & k) == 0;
+                if ((a > bb) == up) {
+                  keys[i] = bb;
+                  keys[l] = a;
+                }
+              }
+            }
+            __syncthreads();
+          }
         }
-        sorted[s0 + j + 1] = key;
+        for (int i = threadIdx.x; i < c; i += blockDim.x) {
+          sorted[s0 + i] = keys[i];
+          first[s0 + i] = (i == 0 || (keys[i] >> 32) != (keys[i - 1] >> 32)) ? 1 : 0;
+        }
+        __syncthreads();
+      } else if (threadIdx.x == 0) {
+        for (int i = 1; i < c; i++) {
+          const int64_t key = sorted[s0 + i];
+          int j = i - 1;
+          while (j >= 0 && sorted[s0 + j] > key) {
+            sorted[s0 + j + 1] = sorted[s0 + j];
+            j--;
+          }
+          sorted[s0 + j + 1] = key;
+        }
+        for (int i = 0; i < c; i++)
+          first[s0 + i] = (i == 0 || (sorted[s0 + i] >> 32) != (sorted[s0 + i - 1] >> 32)) ? 1 : 0;
       }
-      for (int i = 0; i < c; i++)
-        first[s0 + i] = (i == 0 || (sorted[s0 + i] >> 32) != (sorted[s0 + i - 1] >> 32)) ? 1 : 0;
+      __syncthreads();
     }
   }
 }
@@ -364,7 +427,8 @@ extern "C" int ngs_vdedup_sort(const int32_t* vert_ids, int64_t n_keys, const in
   if (n_keys == 0) return NGS_OK;
   cudaStream_t st = (cudaStream_t)s;
   { ngs_count_launch(); vd_scatter_kernel<<<ngs_blocks(n_keys, 256), 256, 0, st>>>(vert_ids, n_keys, bucket_start, bucket_fill, sorted_keys); }
-  { ngs_count_launch(); vd_sort_kernel<<<ngs_blocks(n_buckets * 32, 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
+  { ngs_count_launch(); vd_sort_kernel<<<ngs_blocks(n_buckets, 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
+  { ngs_count_launch(); vd_sort_big_kernel<<<(unsigned)std::min<int64_t>(148 * 8, (n_buckets + 255) / 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
