@@ -18,6 +18,7 @@ is the sum over ranks of reconstructions divided by the slowest rank's time.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -213,10 +214,16 @@ def serving_leg(n_requests=1024, slots=8, plain_every=8):
         l1, s1 = srv.batcher.launches, srv.batcher.batched_systems
         sat = srv.run(reqs, realtime=False)
         sat_s = max(r.done for r in sat)
+        # the same stream at a sustainable rate: arrivals slowed to half the saturated throughput
+        half = 0.5 * (n_requests / sat_s)
+        slow = [dataclasses.replace(r, arrival=r.arrival * 200.0 / half) for r in reqs[:max(64, n_requests // 4)]]
+        low = srv.run(slow, realtime=True)
         waits, peak = srv.adm.waits, srv.adm.peak_in_use
+        direct = srv.batcher.direct_solves
     finally:
         srv.close()
-    errors = sum(r.error is not None for r in rt + sat)
+    errors = sum(r.error is not None for r in rt + sat + low)
+    low_stats = latency_stats(low)
     seq_rps = n_requests / seq_s
     rt_stats, alone = latency_stats(rt), latency_stats(seq)
     return {"requests": n_requests, "slots": slots, "errors": errors,
@@ -231,6 +238,9 @@ def serving_leg(n_requests=1024, slots=8, plain_every=8):
             "speedup_vs_sequential": (n_requests / sat_s) / seq_rps,
             "speedup_vs_sequential_plain_fp64": (n_requests / sat_s) / plain_rps,
             "p99_over_alone_p99": rt_stats["p99_ms"] / alone["p99_ms"],
+            "at_half_saturated_rate": {"offered_rate_rps": half, "requests": len(low), **low_stats,
+                                       "p99_over_alone_p99": low_stats["p99_ms"] / alone["p99_ms"]},
+            "cluster_solves_on_worker_streams": direct,
             "pcg_launches_per_system": (l1 - l0) / max(1, s1 - s0),
             "admission_waits": waits, "peak_admitted_bytes": int(peak),
             "total_points": int(sum(r.xyz.shape[0] for r in reqs))}

@@ -250,8 +250,12 @@ typedef struct ngs_pcg_batch_item {
   int64_t* info_dev;         /* int64[4], as ngs_pcg_solve */
   double* resid_dev;         /* double[2] */
 } ngs_pcg_batch_item;
+/* Co-resident blocks of the cooperative launch; blocks a system takes in it (0: the system is small
+ * enough for one thread-block cluster and is solved by its own cluster launch, alone or in a batch --
+ * ngs_pcg_cluster_size gives the CTAs of that cluster, 0 for the cooperative path). */
 int ngs_pcg_block_capacity(int mode);
 int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode);
+int ngs_pcg_cluster_size(int64_t n, int64_t nnz, int mode);
 int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items, ngs_stream s);
 
 /* ngs_pcg_solve without any workspace from the caller, for callers that cannot allocate device

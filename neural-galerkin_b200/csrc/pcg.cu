@@ -41,6 +41,8 @@ constexpr int PCG_MIN_BLOCKS = 2;      // blocks per SM the register budget is s
 constexpr int PCG_ROW_LANES = 8;       // lanes per row in the SpMV
 constexpr int PCG_ROW_COST = 8;        // work of a row on top of its non-zeros (vector traffic)
 constexpr int PCG_BLOCK_WORK = 16384;  // work (non-zeros + row cost) that justifies one more block
+constexpr int PCG_CLUSTER_MAX = 16;    // CTAs of the largest thread-block cluster a small system gets
+constexpr int PCG_CLUSTER_NEED = 64;   // systems of at most this many blocks' work are solved by a cluster
 
 struct PcgArgs {
   int64_t n;
@@ -229,6 +231,97 @@ NGS_DEV bool plain_barrier(const PcgArgs& a, unsigned bid) {
 
 NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0; }
 
+// Synchronisation of the blocks that solve one system.  GridSync: the blocks of a cooperative
+// launch, through a counter in global memory (bounded waits).  ClusterSync: the CTAs of one
+// thread-block cluster, through the hardware cluster barrier and distributed shared memory -- no
+// spinning, no co-residency requirement beyond the cluster, which the hardware schedules as a unit.
+struct GridSync {
+  const PcgArgs& a;
+  unsigned bid;
+  template <int NV>
+  NGS_DEV bool reduce(const double (&v)[NV], double (&out)[NV]) { return reduce_barrier<NV>(a, bid, v, out); }
+  NGS_DEV bool barrier() { return plain_barrier(a, bid); }
+  NGS_DEV bool late() const { return past_deadline(a); }
+};
+
+NGS_DEV void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+NGS_DEV double ld_dsmem(const double* p, unsigned rank) {
+  uint32_t la = (uint32_t)__cvta_generic_to_shared(p), ra;
+  double v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(rank));
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(ra) : "memory");
+  return v;
+}
+NGS_DEV unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+NGS_DEV unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+
+struct ClusterSync {
+  unsigned rank, size;
+  double* cred;                    // shared [2][4]: this CTA's partial sums, double-buffered
+  double* bcast;                   // shared [4]: the cluster sums, for the CTA's threads
+  int parity;
+  unsigned long long deadline, budget;   // rank 0, thread 0 decides the deadline for everyone
+  bool is_late;
+  template <int NV>
+  NGS_DEV bool reduce(const double (&v)[NV], double (&out)[NV]) {
+    __shared__ double red[NV > 0 ? NV : 1][PCG_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const double t = warp_sum(v[k]);
+      if (lane == 0) red[k][wid] = t;
+    }
+    __syncthreads();
+    double* mine = cred + parity * 4;
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        double t = 0.0;
+        for (int i = 0; i < PCG_THREADS / 32; i++) t += red[k][i];
+        mine[k] = t;
+      }
+      if (rank == 0) {
+        const unsigned long long now = global_ns();
+        if (deadline == 0ull) deadline = now + budget;
+        mine[3] = now > deadline ? 1.0 : 0.0;
+      }
+    }
+    cluster_sync_all();          // every CTA's partials are written
+    if (threadIdx.x == 0) {
+      // the same fixed rank order in every CTA: every CTA gets the same sums, bit for bit
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        double t = 0.0;
+        for (unsigned r = 0; r < size; r++) t += ld_dsmem(mine + k, r);
+        bcast[k] = t;
+      }
+      bcast[3] = ld_dsmem(mine + 3, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) out[k] = bcast[k];
+    is_late = bcast[3] != 0.0;
+    __syncthreads();             // bcast is rewritten by the next reduction
+    parity ^= 1;                 // the other buffer: a CTA may write it while others still read this one
+    return true;
+  }
+  NGS_DEV bool barrier() {
+    cluster_sync_all();
+    return true;
+  }
+  NGS_DEV bool late() const { return is_late; }
+};
+
 template <int MODE>
 struct PcgTypes;
 template <> struct PcgTypes<NGS_PCG_REFERENCE> { using MT = float; using VT = float; using RT = float; using ACC = float; };
@@ -236,9 +329,9 @@ template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = float;
 template <> struct PcgTypes<NGS_PCG_FP64> { using MT = double; using VT = double; using RT = double; using ACC = double; };
 
 // The solve of one system by the blocks bid = 0 .. a.nblocks-1 of a launch (all of them for a
-// single solve, a contiguous range for one system of a batch).
-template <int MODE>
-NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
+// single solve, a contiguous range for one system of a batch, the CTAs of one cluster).
+template <int MODE, typename Sync>
+NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   using MT = typename PcgTypes<MODE>::MT;
   using VT = typename PcgTypes<MODE>::VT;
   using RT = typename PcgTypes<MODE>::RT;
@@ -289,7 +382,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
     s[i] = (VT)0;
     part[0] += (double)bi * (double)bi;
   }
-  if (!reduce_barrier<3>(a, bid, part, res)) return;
+  if (!sy.template reduce<3>(part, res)) return;
   if (res[1] > 0.0) {                                    // every block sees the same flag: no copy was issued
     if (bid == 0 && threadIdx.x == 0) {
       a.info[0] = 0;
@@ -305,7 +398,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
     part[0] += (double)r[i] * (double)u[i];
     part[2] += (double)r[i] * (double)r[i];
   }
-  if (!reduce_barrier<3>(a, bid, part, res)) return;
+  if (!sy.template reduce<3>(part, res)) return;
   double gamma = res[0], delta = res[1], rho = res[2];
   double alpha = delta != 0.0 ? gamma / delta : 0.0, beta = 0.0;
   int it = 0, replacements = 0;
@@ -314,7 +407,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
   bool converged = sqrt(rho) <= atol || bnorm == 0.0, timed_out = false;
   const int cap = (a.max_iter >= 0 && a.max_iter < NGS_PCG_ITER_CAP) ? a.max_iter : NGS_PCG_ITER_CAP;
   while (!converged && it < cap) {
-    if (past_deadline(a)) { timed_out = true; break; }
+    if (sy.late()) { timed_out = true; break; }
     const bool replace =
         (MODE == NGS_PCG_MIXED && a.replace_every > 0 && (it + 1) % a.replace_every == 0) ||
         (MODE == NGS_PCG_REFERENCE && a.replace_every > 0 && (it + 1) % sqrt_n == 0);
@@ -338,17 +431,17 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
     }
     if (replace) {
       // residual replacement: r = b - A x (FP64 matrix in MIXED mode, the FP32 one in REFERENCE mode)
-      if (!plain_barrier(a, bid)) return;
+      if (!sy.barrier()) return;
       double rr = 0.0;
       spmv_true(rr);
       part[2] = rr;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       replacements++;
     }
-    if (!plain_barrier(a, bid)) return;
+    if (!sy.barrier()) return;
     // phase B: w = A u and (w, u)
     spmv_w(part[1]);
-    if (!reduce_barrier<3>(a, bid, part, res)) return;
+    if (!sy.template reduce<3>(part, res)) return;
     it++;
     const double gamma_new = res[0];
     delta = res[1];
@@ -356,14 +449,14 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
     if (sqrt(rho) <= target) {
       if (MODE != NGS_PCG_MIXED) { converged = true; break; }
       // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
-      if (!plain_barrier(a, bid)) return;
+      if (!sy.barrier()) return;
       part[0] = part[1] = part[2] = 0.0;
       spmv_true(part[2]);
       replacements++;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
-      if (!plain_barrier(a, bid)) return;
+      if (!sy.barrier()) return;
       spmv_w(part[1]);
-      if (!reduce_barrier<3>(a, bid, part, res)) return;
+      if (!sy.template reduce<3>(part, res)) return;
       rho = res[2];
       if (sqrt(rho) <= atol) { converged = true; break; }
       gamma = res[0];
@@ -391,7 +484,17 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid) {
 
 template <int MODE>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_kernel(const __grid_constant__ PcgArgs a) {
-  pcg_body<MODE>(a, blockIdx.x);
+  GridSync sy{a, blockIdx.x};
+  pcg_body<MODE>(a, blockIdx.x, sy);
+}
+
+// A small system solved by one thread-block cluster (a.nblocks CTAs, the whole grid).
+template <int MODE>
+__global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_cluster_kernel(const __grid_constant__ PcgArgs a) {
+  __shared__ double cred[8], bcast[4];
+  ClusterSync sy{cluster_rank(), cluster_size(), cred, bcast, 0, 0ull, a.budget_ns, false};
+  pcg_body<MODE>(a, sy.rank, sy);
+  cluster_sync_all();            // no CTA exits while another may still read its shared memory
 }
 
 // A batch of independent systems in one cooperative launch: system k owns the blocks
@@ -412,7 +515,8 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_batch_kernel(
     const int mid = (lo + hi + 1) >> 1;
     if (b.start[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
   }
-  pcg_body<MODE>(b.sys[lo], blockIdx.x - b.start[lo]);
+  GridSync sy{b.sys[lo], blockIdx.x - b.start[lo]};
+  pcg_body<MODE>(b.sys[lo], blockIdx.x - b.start[lo], sy);
 }
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -466,9 +570,90 @@ extern "C" int ngs_pcg_block_capacity(int mode) {
   return capacity_of(mode);
 }
 
+// Largest cluster of pcg_cluster_kernel<MODE> the current device can run (cached per device).
+template <int MODE>
+static int pcg_cluster_limit() {
+  static int cached[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && cached[dev] != 0) return cached[dev] > 0 ? cached[dev] : 0;
+  int limit = 0;
+  if (cudaFuncSetAttribute(pcg_cluster_kernel<MODE>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+      cudaSuccess) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(PCG_CLUSTER_MAX);
+    lc.blockDim = dim3(PCG_THREADS);
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = PCG_CLUSTER_MAX;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    lc.attrs = &attr;
+    lc.numAttrs = 1;
+    if (cudaOccupancyMaxPotentialClusterSize(&limit, (const void*)pcg_cluster_kernel<MODE>, &lc) != cudaSuccess)
+      limit = 0;
+  }
+  cudaGetLastError();   // a refused query leaves no sticky error: the cooperative path is used instead
+  if (limit > PCG_CLUSTER_MAX) limit = PCG_CLUSTER_MAX;
+  if (dev >= 0 && dev < 64) cached[dev] = limit > 0 ? limit : -1;
+  return limit;
+}
+
+static int cluster_limit_of(int mode) {
+  if (mode == NGS_PCG_REFERENCE) return pcg_cluster_limit<NGS_PCG_REFERENCE>();
+  if (mode == NGS_PCG_MIXED) return pcg_cluster_limit<NGS_PCG_MIXED>();
+  return pcg_cluster_limit<NGS_PCG_FP64>();
+}
+
+// CTAs of the cluster that solves a system of this size, or 0 for the cooperative grid path: a
+// system of at most PCG_CLUSTER_NEED blocks' work goes to one cluster of up to PCG_CLUSTER_MAX CTAs
+// (unless the caller asked for a block count).
+static int pcg_cluster_for(int64_t n, int64_t nnz, int blocks_req, int limit) {
+  if (blocks_req > 0 || limit < 1) return 0;
+  const int64_t need = (nnz + (int64_t)PCG_ROW_COST * n + PCG_BLOCK_WORK - 1) / PCG_BLOCK_WORK;
+  if (need > PCG_CLUSTER_NEED) return 0;
+  return (int)(need < 1 ? 1 : (need < limit ? need : limit));
+}
+
+extern "C" int ngs_pcg_cluster_size(int64_t n, int64_t nnz, int mode) {
+  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0) return 0;
+  return pcg_cluster_for(n, nnz, 0, cluster_limit_of(mode));
+}
+
 extern "C" int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode) {
   if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0) return 0;
+  if (ngs_pcg_cluster_size(n, nnz, mode) > 0) return 0;      // solved by a cluster, outside the grid
   return (int)pcg_blocks_for(n, nnz, 0, capacity_of(mode));
+}
+
+static void* pcg_cluster_kernel_of(int mode) {
+  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_cluster_kernel<NGS_PCG_REFERENCE>;
+  if (mode == NGS_PCG_MIXED) return (void*)pcg_cluster_kernel<NGS_PCG_MIXED>;
+  return (void*)pcg_cluster_kernel<NGS_PCG_FP64>;
+}
+
+// One cluster of `csize` CTAs solves the system (an ordinary launch: the hardware places the whole
+// cluster at once, so the cluster barrier needs no cooperative launch).
+static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
+  a.nblocks = (unsigned int)csize;
+  cudaMemsetAsync(a.count, 0, 8 * sizeof(unsigned int), st);
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3((unsigned)csize);
+  lc.blockDim = dim3(PCG_THREADS);
+  lc.dynamicSmemBytes = 0;
+  lc.stream = st;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = (unsigned)csize;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  lc.attrs = &attr;
+  lc.numAttrs = 1;
+  void* args[] = {&a};
+  ngs_count_launch();
+  const cudaError_t e = cudaLaunchKernelExC(&lc, pcg_cluster_kernel_of(mode), args);
+  if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  return NGS_OK;
 }
 
 // Validate one system, carve its workspace and fill the kernel arguments (nblocks left 0).
@@ -547,6 +732,8 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   const int rc = prepare_pcg(sys, cfg, ws, ws_bytes, info_dev, resid_dev, st, a);
   if (rc == 1) return NGS_OK;
   if (rc != NGS_OK) return rc;
+  const int csize = pcg_cluster_for(a.n, a.nnz, cfg->blocks, cluster_limit_of(cfg->mode));
+  if (csize > 0) return launch_cluster(a, cfg->mode, csize, st);
   const int cap = capacity_of(cfg->mode);
   if (cap < 1) return NGS_ERR_CUDA;
   const int64_t blocks = pcg_blocks_for(a.n, a.nnz, cfg->blocks, cap);
@@ -572,8 +759,12 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
   const int cap = capacity_of(mode);
   if (cap < 1) return NGS_ERR_CUDA;
   static thread_local PcgBatch b;          // 15 KB: kept off the stack
+  static thread_local PcgArgs small[NGS_PCG_BATCH_MAX];
+  static thread_local int small_size[NGS_PCG_BATCH_MAX];
   b.nsys = 0;
+  int nsmall = 0;
   unsigned int total = 0;
+  const int climit = cluster_limit_of(mode);
   // validate and size everything before the first memset, so that a rejected batch touches nothing
   for (int k = 0; k < n_items; k++) {
     const ngs_pcg_batch_item& it = items[k];
@@ -581,6 +772,12 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     const int rc = prepare_pcg(&it.sys, &it.cfg, it.ws, it.ws_bytes, it.info_dev, it.resid_dev, st, a);
     if (rc == 1) continue;
     if (rc != NGS_OK) return rc;
+    const int csize = pcg_cluster_for(a.n, a.nnz, it.cfg.blocks, climit);
+    if (csize > 0) {                         // solved by its own cluster, as it would be alone
+      small[nsmall] = a;
+      small_size[nsmall++] = csize;
+      continue;
+    }
     const int64_t blocks = pcg_blocks_for(a.n, a.nnz, it.cfg.blocks, cap);
     if (blocks < 1) return NGS_ERR_INVALID_ARG;
     if (total + blocks > (unsigned)cap) return NGS_ERR_INVALID_ARG;   // not co-resident: split the batch
@@ -588,6 +785,10 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     b.start[b.nsys] = total;
     b.sys[b.nsys++] = a;
     total += (unsigned)blocks;
+  }
+  for (int k = 0; k < nsmall; k++) {
+    const int rc = launch_cluster(small[k], mode, small_size[k], st);
+    if (rc != NGS_OK) return rc;
   }
   if (b.nsys == 0) return NGS_OK;
   b.start[b.nsys] = total;

@@ -94,6 +94,7 @@ _SIGS = {
     "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
     "ngs_pcg_block_capacity": ([C.c_int], C.c_int),
     "ngs_pcg_blocks": ([i64, i64, C.c_int], C.c_int),
+    "ngs_pcg_cluster_size": ([i64, i64, C.c_int], C.c_int),
     "ngs_pcg_solve_batch": ([C.POINTER(PcgBatchItem), C.c_int, vp], C.c_int),
     "ngs_pcg_noalloc_max_rows": ([], i64),
     "ngs_pcg_solve_noalloc": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, vp, vp], C.c_int),
@@ -133,7 +134,11 @@ def load():
     if _lib is None:
         if not LIB_PATH.exists():
             raise RuntimeError(f"libngs.so not found at {LIB_PATH}; build it with neural-galerkin_b200/build.py")
-        lib = C.CDLL(str(LIB_PATH))
+        # PyDLL: the interpreter lock is kept across calls.  Every entry point only enqueues work on
+        # a stream and returns in microseconds; releasing and re-acquiring the lock around each of
+        # the few hundred calls of a reconstruction makes concurrent host threads (the serving
+        # workers) queue for the lock at every call.
+        lib = C.PyDLL(str(LIB_PATH))
         for name, (args, ret) in _SIGS.items():
             fn = getattr(lib, name)
             fn.argtypes, fn.restype = args, ret

@@ -6,9 +6,9 @@ and runs it on its own CUDA stream through the device-resident pipeline (tree, a
 dual marching cubes, mesh copied back to pinned host memory).  Requests in flight overlap on the
 device.  Their per-level PCG solves do not run as separate launches: a batcher collects the solves
 that are ready, from every stream, and issues them as one cooperative launch
-(``ngs_pcg_solve_batch``) -- small systems that would each leave most SMs idle share the GPU,
-and each system keeps the block count of its solo solve, so its result is bit-identical to
-solving it alone.
+(``ngs_pcg_solve_batch``), each system keeping the block count of its solo solve, so that its
+result is bit-identical to solving it alone.  Systems small enough for one thread-block cluster
+skip the batcher: their cluster solve runs on the worker's own stream, concurrently with the rest.
 
 Nothing here changes what a reconstruction computes: a request's mesh is the one
 ``jspsr.reconstruct`` returns for the same input, up to the order of floating-point atomics in
@@ -150,6 +150,7 @@ class SolveBatcher:
         self.stop = False
         self.launches = 0
         self.batched_systems = 0
+        self.direct_solves = 0
         self.inflight = None
         self.lib = L.load()
         self.thread = threading.Thread(target=self._loop, name="ngs-solve-batcher", daemon=True)
@@ -158,6 +159,13 @@ class SolveBatcher:
     # called from a worker thread, on the worker's current stream
     def submit(self, rec, lv, d, item):
         import torch
+        if self.lib.ngs_pcg_cluster_size(item.sys.n, item.sys.nnz, item.cfg.mode) > 0:
+            # small system: one thread-block cluster solves it on the worker's own stream, next to
+            # everything else in flight -- nothing to batch, nothing to wait for
+            L.call("ngs_pcg_solve", L.C.byref(item.sys), L.C.byref(item.cfg), item.ws, item.ws_bytes, item.info_dev,
+                   item.resid_dev, L.stream())
+            self.direct_solves += 1
+            return
         ready = torch.cuda.Event()
         ready.record()
         t = dict(item=item, ready=ready, done=None, rc=None, ev=threading.Event(),
