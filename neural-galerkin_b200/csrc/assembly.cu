@@ -307,10 +307,17 @@ __global__ void correction_kernel(const int32_t* __restrict__ fc, int64_t nf, in
 extern "C" int ngs_correction_stiffness(const int32_t* fine_coords, int64_t n_fine, int fine_stride, ngs_grid cg,
                                         const float* x_coarse, const double* tab_c, const double* tab_g, int tab_len,
                                         double* rhs, ngs_stream s) {
-  if (n_fine < 0 || fine_stride <= 0 || cg.stride <= fine_stride || tab_len <= 0 || tab_len > 4096) return NGS_ERR_INVALID_ARG;
+  // tables of 3M + 2 entries each: level ratios M up to 2^12 (13 levels) fit one block's shared memory
+  if (n_fine < 0 || fine_stride <= 0 || cg.stride <= fine_stride || tab_len <= 0 || tab_len > 12290)
+    return NGS_ERR_INVALID_ARG;
   if (n_fine == 0) return NGS_OK;
   if (!fine_coords || !cg.words || !x_coarse || !tab_c || !tab_g || !rhs) return NGS_ERR_INVALID_ARG;
-  { ngs_count_launch(); correction_kernel<<<ngs_blocks(n_fine, 128), 128, 2 * tab_len * sizeof(double), (cudaStream_t)s>>>(
+  const size_t smem = 2 * (size_t)tab_len * sizeof(double);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(correction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return ngs_set_cuda_error(e);
+  }
+  { ngs_count_launch(); correction_kernel<<<ngs_blocks(n_fine, 128), 128, smem, (cudaStream_t)s>>>(
       fine_coords, n_fine, fine_stride, cg, x_coarse, tab_c, tab_g, tab_len, rhs); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;

@@ -502,15 +502,17 @@ class Reconstruction:
             L.call("ngs_expand_cells", L.ptr(base[d]), base[d].shape[0], n_upsample, self.levels[d].stride, evs,
                    L.ptr(epb[starts[d]:]), L.ptr(pos[starts[d]:]), st)
         # dual centres: unique corners of all expanded cells
-        lo = np.full(3, np.iinfo(np.int64).max)
-        hi = np.full(3, np.iinfo(np.int64).min)
+        # box of the corners actually present (the cells' extent, not the levels' padded boxes: with
+        # many levels the coarse boxes would make the bitmap far larger than the surface needs)
+        ext = []
         for d in range(max_depth):
-            s = self.levels[d].stride
-            g = self.levels[d].grid
-            glo = np.array(g.origin[:], dtype=np.int64)
-            ghi = glo + (np.array(g.dims[:], dtype=np.int64) - 1) * s
-            lo = np.minimum(lo, n_upsample * (glo - 2 * s))
-            hi = np.maximum(hi, n_upsample * (ghi + 3 * s))
+            c = epb[starts[d]:starts[d] + counts[d]]
+            if counts[d] == 0:
+                continue
+            ext.append(torch.cat([c.min(0).values.long(), c.max(0).values.long() + self.levels[d].stride]))
+        ext = torch.stack(ext).cpu().numpy()
+        lo = ext[:, :3].min(0)
+        hi = ext[:, 3:].max(0)
         dg, dw = L.make_grid(lo, (hi - lo) + 1, 1, dev)
         offs = L.device_table("conform_offsets", lambda: CONFORM_OFFSETS, dev)
         for d in range(max_depth):
