@@ -374,7 +374,7 @@ def main():
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
     tf = ROOT / "profiles" / "pcg_mixed_superquadrics300k_traffic.txt"
-    if tf.exists():
+    if tf.exists() and W["workload"] == "superquadrics-300k":    # the capture is of this workload
         for line in tf.read_text().splitlines():
             if line.startswith("dram_bytes_per_iteration_level0:"):
                 traffic = float(line.split(":")[1]) * iters0

@@ -160,6 +160,8 @@ class Reconstruction:
         self.profile_pcg = False
         self._pcg_events = {}
         self.solve_hook = None     # callable(rec, level, d, item): hands the level's PCG to a batcher
+        # largest dual-grid rank bitmap (16-byte words) before the mesh switches to sorted keys
+        self.dual_grid_max_words = 1 << 27
 
     def _mark(self, name):
         if self.t is not None:
@@ -513,19 +515,36 @@ class Reconstruction:
         ext = torch.stack(ext).cpu().numpy()
         lo = ext[:, :3].min(0)
         hi = ext[:, 3:].max(0)
-        dg, dw = L.make_grid(lo, (hi - lo) + 1, 1, dev)
+        dims = (hi - lo) + 1
         offs = L.device_table("conform_offsets", lambda: CONFORM_OFFSETS, dev)
-        for d in range(max_depth):
-            L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
-                   self.levels[d].stride, st)
-        dcount = torch.empty(1, dtype=torch.int64, device=dev)
-        self._dual_ws = L.grid_finalize(dg, dw, dcount)
-        nd = int(dcount.item())
-        acc = torch.zeros((nd, 8, 2), dtype=torch.int32, device=dev)
-        cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
-        for d in range(max_depth):
-            L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride, d,
-                   int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
+        box_words = int(dims[0]) * int(dims[1]) * ((int(dims[2]) + 63) // 64)
+        if box_words <= self.dual_grid_max_words:
+            # rank bitmap over the box: dual centres ranked without a sort
+            dg, dw = L.make_grid(lo, dims, 1, dev)
+            for d in range(max_depth):
+                L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
+                       self.levels[d].stride, st)
+            dcount = torch.empty(1, dtype=torch.int64, device=dev)
+            self._dual_ws = L.grid_finalize(dg, dw, dcount)
+            nd = int(dcount.item())
+            acc = torch.zeros((nd, 8, 2), dtype=torch.int32, device=dev)
+            cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
+            for d in range(max_depth):
+                L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride, d,
+                       int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
+        else:
+            # deep hierarchies: the coarse cells stretch the box far beyond the surface, so the
+            # dual centres are de-duplicated by a sort of packed corner keys and found through the
+            # key table instead (the reference's own route, reconstructor.py:347-357)
+            if np.any(dims >= (1 << 21)):
+                raise ValueError(f"mesh domain of {dims.tolist()} cells exceeds 2^21 cells per axis")
+            nd, table = self._dual_centres_by_sort(epb, starts, counts, max_depth, lo, offs)
+            acc = torch.zeros((nd, 8, 2), dtype=torch.int32, device=dev)
+            cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
+            for d in range(max_depth):
+                L.call("ngs_dual_mc_indices_hash", L.C.byref(table.table), L.ptr(epb[starts[d]:]), counts[d],
+                       self.levels[d].stride, d, int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
+            self._dual_ws = table
         keep = torch.empty(nd, dtype=torch.int32, device=dev)
         L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
         koff, ktot = L.scan(keep)
@@ -564,6 +583,22 @@ class Reconstruction:
         self.mesh_info = dict(n_primal=total, n_dual=nd, n_cubes=m, max_depth=max_depth, acc=acc_c, values=vals,
                               positions=pos, counts=counts)
         return verts, faces.view(-1, 3)
+
+    def _dual_centres_by_sort(self, epb, starts, counts, max_depth, lo, offs):
+        """Unique corners of the expanded cells, in lexicographic order, and a key table over them."""
+        from ..ext import HashLookupData, hash_cuda
+        lo_t = torch.as_tensor(lo, dtype=torch.int64, device=self.dev)
+        keys = []
+        for d in range(max_depth):
+            c = epb[starts[d]:starts[d] + counts[d]]
+            if c.shape[0] == 0:
+                continue
+            corners = (c[:, None, :].long() + offs.long()[None] * self.levels[d].stride).reshape(-1, 3) - lo_t
+            keys.append((corners[:, 0] << 42) | (corners[:, 1] << 21) | corners[:, 2])
+        uk = torch.unique(torch.cat(keys))           # sorted: packed keys order like (x, y, z)
+        mask = (1 << 21) - 1
+        dual = (torch.stack([uk >> 42, (uk >> 21) & mask, uk & mask], 1) + lo_t).int()
+        return int(uk.numel()), HashLookupData(hash_cuda(dual), None, False)
 
     def run(self, n_upsample: int = 2):
         self.build_tree().assemble().solve()

@@ -155,3 +155,24 @@ def test_empty_level_raises():
     xyz, nrm = synthetic.torus(n=2000)
     with pytest.raises(ValueError, match="empty"):
         jspsr.reconstruct(xyz, nrm, 1.0 / 128, depth=3, min_density=32.0)
+
+
+@pytest.mark.parametrize("name", ["torus_adaptive", "sq_noisy"])
+def test_sorted_key_dual_centres_match_bitmap(cases, name):
+    """Deep hierarchies de-duplicate dual centres by sorting packed corner keys instead of a rank
+    bitmap over the box; forcing that route gives the same dual grid and mesh."""
+    from jspsr.core.pipeline import Reconstruction
+    g, _, _ = cases[name]
+    vs, depth, md, alpha = g["params"]
+    xyz = torch.from_numpy(g["xyz"]).cuda()
+    nrm = torch.from_numpy(g["nrm"]).cuda()
+    out = []
+    rec = Reconstruction(xyz, nrm, vs, int(depth), md, alpha, solver="pcg-mixed@tol=1e-9")
+    rec.build_tree().assemble().solve()
+    for max_words in (1 << 27, 0):
+        rec.dual_grid_max_words = max_words
+        v, f = rec.extract_mesh()
+        out.append((rec.mesh_info["acc"].cpu().numpy(), v.cpu().numpy(), f.cpu().numpy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.abs(out[0][1] - out[1][1]).max() <= 1e-5
