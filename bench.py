@@ -79,6 +79,23 @@ def cpu_reconstruct(xyz, nrm):
                             WORKLOAD["screen_alpha"], cg_tol=1e-7)
 
 
+# ----------------------------------------------------------------------------- replicas
+def slowest_rank_ms(ms: float, world: int, device: str) -> float:
+    """The timed region's duration on the slowest rank (every rank calls this, in the same order)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(ms: float, world: int, steps: int) -> float:
+    """Reconstructions per second of the whole job: every rank ran ``steps`` independent replicas."""
+    return world * steps / (ms / 1e3)
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -323,12 +340,8 @@ def main():
         torch.cuda.synchronize()
         barrier()
     launches = lib.ngs_launch_count() - l0
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = slowest_rank_ms(t0.elapsed_time(t1), world, "cuda")
+    value = job_throughput(ms, world, args.steps)
 
     # ---------------------------------------------------------------- end to end through the public API
     xyz_h = torch.from_numpy(xyz).pin_memory()
@@ -350,12 +363,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "recon/s",
+    e2e_ms = slowest_rank_ms(e0.elapsed_time(e1), world, "cuda")
+    e2e = {"value": job_throughput(e2e_ms, world, args.steps), "unit": "recon/s",
            "h2d_bytes_per_step": int(xyz.nbytes + nrm.nbytes), "d2h_bytes_per_step": int(d2h)}
 
     # ---------------------------------------------------------------- roofline of the dominant kernel (level-0 PCG)
