@@ -150,6 +150,12 @@ int ngs_point_field(const int32_t* rows, const float* phi, int64_t n, const floa
  * positions, accumulated into out. ref: jspsr/core/hashtree.py:157-192 */
 int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv_vs, double vs, const float* x, int grad,
                    float* out, ngs_stream s);
+/* The field of all levels (the sum of ngs_eval_field over them, added in level order) in one pass:
+ * grids[l] and x[l] of n_levels <= NGS_MAX_FIELD_LEVELS levels; accumulates into out like
+ * ngs_eval_field.  (evaluate_raw_chi, reconstructor.py:197-226, as one launch.) */
+#define NGS_MAX_FIELD_LEVELS 16
+int ngs_eval_field_levels(const ngs_grid* grids, const float* const* x, int n_levels, const float* pos, int64_t n,
+                          float inv_vs, double vs, int grad, float* out, ngs_stream s);
 /* sum_p w[p] * v[p] and sum_p w[p] into sums_dev double[2] (mean-chi level set). */
 int ngs_weighted_sum(const float* v, const float* w, int64_t n, double* sums_dev, ngs_stream s);
 
@@ -167,6 +173,13 @@ int ngs_stencil_fill(ngs_grid g, const int32_t* coords, int64_t V, const uint32_
 /* vals[slot(a, b)] += scale * w[p] * phi[p,a] * phi[p,b] over all point pairs (w NULL = 1). */
 int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n, const float* w, const uint32_t* masks,
                     const int64_t* rowptr, double scale, double* vals, ngs_stream s);
+/* ngs_screen_gram with the points grouped by cell: order = the point ids sorted by keys (keys[i] is
+ * the key of point order[i]: first present row of the point's 27 * 27 + that row's position, or -1
+ * for a point with no voxel at this level).  One atomic per (cell, row, column) instead of per point;
+ * the same sums up to the order of FP64 additions.  No counterpart in the reference. */
+int ngs_screen_gram_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w, const int64_t* order,
+                            const int64_t* keys, const uint32_t* masks, const int64_t* rowptr, double scale,
+                            double* vals, ngs_stream s);
 /* rhs[row] += scale * sum_p w[p] * phi[p,k]  (screening target term). */
 int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, const float* w, double scale, double* rhs,
                    ngs_stream s);

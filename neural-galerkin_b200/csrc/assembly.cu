@@ -128,6 +128,58 @@ extern "C" int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n,
   return NGS_OK;
 }
 
+// The same sum with the points grouped by their 27-voxel neighbourhood: points in one cell share all
+// 27 rows, so their outer products are summed in registers (lane a keeps row a's 27 sums) and each
+// (row, column) slot takes one atomic per cell instead of one per point.  order / keys: the points
+// sorted by key = first present row * 27 + its position (-1: no voxel), a key that fixes the cell.
+// One warp per sorted position; the warp at the first position of a run of equal keys does the run.
+__global__ void screen_gram_grouped_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi,
+                                           int64_t n, const float* __restrict__ w, const int64_t* __restrict__ order,
+                                           const int64_t* __restrict__ keys, const uint4* __restrict__ masks,
+                                           const int64_t* __restrict__ rowptr, double scale,
+                                           double* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ngs_gtid() >> 5; i < n; i += warps) {
+    const int64_t key = keys[i];
+    if (key < 0 || (i > 0 && keys[i - 1] == key)) continue;      // warp-uniform
+    const int64_t p0 = order[i];
+    const int32_t ra = lane < 27 ? rows[p0 * 27 + lane] : -1;
+    double acc[27];
+#pragma unroll
+    for (int b = 0; b < 27; b++) acc[b] = 0.0;
+    for (int64_t j = i; j < n && keys[j] == key; j++) {
+      const int64_t p = order[j];
+      const float pa = lane < 27 ? phi[p * 27 + lane] : 0.f;
+      const double sa = (double)(w ? w[p] : 1.f) * (double)pa;
+#pragma unroll
+      for (int b = 0; b < 27; b++) acc[b] += sa * (double)__shfl_sync(0xffffffffu, pa, b);
+    }
+    const uint4 m = ra >= 0 ? masks[ra] : make_uint4(0, 0, 0, 0);
+    const int64_t base = ra >= 0 ? rowptr[ra] : 0;
+    const int ax = lane / 9, ay = (lane / 3) % 3, az = lane % 3;
+#pragma unroll
+    for (int b = 0; b < 27; b++) {
+      const int32_t rb = __shfl_sync(0xffffffffu, ra, b);      // all 32 lanes take part in the shuffle
+      if (ra < 0 || rb < 0) continue;
+      const int bx = b / 9, by = (b / 3) % 3, bz = b % 3;
+      const int o = (bx - ax + 2) * 25 + (by - ay + 2) * 5 + (bz - az + 2);
+      atomicAdd(vals + base + popc_below(m, o), scale * acc[b]);
+    }
+  }
+}
+
+extern "C" int ngs_screen_gram_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w,
+                                       const int64_t* order, const int64_t* keys, const uint32_t* masks,
+                                       const int64_t* rowptr, double scale, double* vals, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !phi || !order || !keys || !masks || !rowptr || !vals))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  { ngs_count_launch(); screen_gram_grouped_kernel<<<ngs_blocks(n * 32, 256), 256, 0, (cudaStream_t)s>>>(
+      rows, phi, n, w, order, keys, reinterpret_cast<const uint4*>(masks), rowptr, scale, vals); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
 __global__ void screen_rhs_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi, int64_t n,
                                   const float* __restrict__ w, const float* __restrict__ field, double scale,
                                   double* __restrict__ rhs) {

@@ -321,37 +321,84 @@ extern "C" int ngs_point_field(const int32_t* rows, const float* phi, int64_t n,
   return NGS_OK;
 }
 
-// Field value / gradient at arbitrary positions, accumulated into out
-// (hashtree.py:157-192, bezier_tensor.py:56-73: the gradient is per finest-voxel unit / stride).
-__global__ void eval_field_kernel(ngs_grid g, const float* __restrict__ pos, int64_t n, float inv_vs, double vs,
-                                  const float* __restrict__ x, int grad, float* __restrict__ out) {
+// Rows of the three cells (x, y, z + t * stride), t = 0, 1, 2, or -1 where absent: the three share
+// one or two bitmap words, loaded once each.
+NGS_DEV void grid_rows_z3(const ngs_grid& g, int x, int y, int z, int32_t (&r)[3]) {
+  r[0] = r[1] = r[2] = -1;
+  const int dx = x - g.origin[0], dy = y - g.origin[1], dz = z - g.origin[2];
+  if ((dx | dy) < 0) return;
+  const int i = dx >> g.log2_stride, j = dy >> g.log2_stride;
+  if (i >= g.dims[0] || j >= g.dims[1]) return;
+  const uint4* row = reinterpret_cast<const uint4*>(g.words) + ((int64_t)i * g.dims[1] + j) * g.zwords;
+  const int k0 = dz >> g.log2_stride;               // arithmetic shift: floor for cells below the box
+  int have = -1;
+  uint4 v = make_uint4(0, 0, 0, 0);
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    const int k = k0 + t;
+    if (k < 0 || k >= g.dims[2]) continue;
+    const int w = k >> 6;
+    if (w != have) {
+      v = __ldg(row + w);
+      have = w;
+    }
+    const unsigned long long bits = (unsigned long long)v.z | ((unsigned long long)v.w << 32);
+    const int b = k & 63;
+    if ((bits >> b) & 1ull) r[t] = (int32_t)(v.x + (unsigned)__popcll(bits & ((1ull << b) - 1ull)));
+  }
+}
+
+// One level's field (or gradient) at a point: 27 basis functions around it (hashtree.py:157-192,
+// bezier_tensor.py:56-73: the gradient is per finest-voxel unit / stride).  All nine bitmap probes
+// are issued before the coefficient gathers.
+NGS_DEV void level_field(const ngs_grid& g, const float* p, float inv_vs, double vs, const float* __restrict__ x,
+                         int grad, float& v, float& gx, float& gy, float& gz) {
   const float inv_s = 1.0f / (float)g.stride;
-  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
-    const PointNbr nb = point_nbr(pos + p * 3, inv_vs, vs, g.stride);
-    float b[3][3], db[3][3];
+  const PointNbr nb = point_nbr(p, inv_vs, vs, g.stride);
+  float b[3][3], db[3][3];
 #pragma unroll
-    for (int a = 0; a < 3; a++)
+  for (int a = 0; a < 3; a++)
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        b[a][k] = bspline(nb.rel[a][k]);
-        db[a][k] = bspline_d(nb.rel[a][k]) * inv_s;
-      }
-    float v = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    for (int kx = 0; kx < 3; kx++)
-      for (int ky = 0; ky < 3; ky++)
-        for (int kz = 0; kz < 3; kz++) {
-          const int64_t r = grid_row(g, nb.q[0] + (kx - 1) * g.stride, nb.q[1] + (ky - 1) * g.stride,
-                                     nb.q[2] + (kz - 1) * g.stride);
-          if (r < 0) continue;
-          const float xr = x[r];
-          if (!grad) {
-            v += b[0][kx] * b[1][ky] * b[2][kz] * xr;
-          } else {
-            gx += db[0][kx] * b[1][ky] * b[2][kz] * xr;
-            gy += b[0][kx] * db[1][ky] * b[2][kz] * xr;
-            gz += b[0][kx] * b[1][ky] * db[2][kz] * xr;
-          }
+    for (int k = 0; k < 3; k++) {
+      b[a][k] = bspline(nb.rel[a][k]);
+      db[a][k] = bspline_d(nb.rel[a][k]) * inv_s;
+    }
+  int32_t rows[3][3][3];
+#pragma unroll
+  for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+    for (int ky = 0; ky < 3; ky++)
+      grid_rows_z3(g, nb.q[0] + (kx - 1) * g.stride, nb.q[1] + (ky - 1) * g.stride, nb.q[2] - g.stride, rows[kx][ky]);
+  float lv = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+#pragma unroll
+  for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+    for (int ky = 0; ky < 3; ky++)
+#pragma unroll
+      for (int kz = 0; kz < 3; kz++) {
+        const int32_t r = rows[kx][ky][kz];
+        if (r < 0) continue;
+        const float xr = x[r];
+        if (!grad) {
+          lv += b[0][kx] * b[1][ky] * b[2][kz] * xr;
+        } else {
+          lx += db[0][kx] * b[1][ky] * b[2][kz] * xr;
+          ly += b[0][kx] * db[1][ky] * b[2][kz] * xr;
+          lz += b[0][kx] * b[1][ky] * db[2][kz] * xr;
         }
+      }
+  v = lv;
+  gx = lx;
+  gy = ly;
+  gz = lz;
+}
+
+// Field value / gradient at arbitrary positions, accumulated into out
+__global__ void __launch_bounds__(128, 6) eval_field_kernel(ngs_grid g, const float* __restrict__ pos, int64_t n, float inv_vs, double vs,
+                                  const float* __restrict__ x, int grad, float* __restrict__ out) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    float v, gx, gy, gz;
+    level_field(g, pos + p * 3, inv_vs, vs, x, grad, v, gx, gy, gz);
     if (!grad) {
       out[p] += v;
     } else {
@@ -360,6 +407,60 @@ __global__ void eval_field_kernel(ngs_grid g, const float* __restrict__ pos, int
       out[p * 3 + 2] += gz;
     }
   }
+}
+
+// All levels in one pass: the point is read once and out written once; the per-level terms are
+// added in level order, as the per-level launches would add them.
+struct FieldLevels {
+  ngs_grid g[NGS_MAX_FIELD_LEVELS];
+  const float* x[NGS_MAX_FIELD_LEVELS];
+  int n;
+};
+
+__global__ void __launch_bounds__(128, 6) eval_field_levels_kernel(const __grid_constant__ FieldLevels fl, const float* __restrict__ pos,
+                                         int64_t n, float inv_vs, double vs, int grad, float* __restrict__ out) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    const float q[3] = {pos[p * 3], pos[p * 3 + 1], pos[p * 3 + 2]};
+    float sv = grad ? 0.f : out[p];
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    if (grad) {
+      sx = out[p * 3];
+      sy = out[p * 3 + 1];
+      sz = out[p * 3 + 2];
+    }
+    for (int l = 0; l < fl.n; l++) {
+      float v, gx, gy, gz;
+      level_field(fl.g[l], q, inv_vs, vs, fl.x[l], grad, v, gx, gy, gz);
+      sv += v;
+      sx += gx;
+      sy += gy;
+      sz += gz;
+    }
+    if (!grad) {
+      out[p] = sv;
+    } else {
+      out[p * 3] = sx;
+      out[p * 3 + 1] = sy;
+      out[p * 3 + 2] = sz;
+    }
+  }
+}
+
+extern "C" int ngs_eval_field_levels(const ngs_grid* grids, const float* const* x, int n_levels, const float* pos,
+                                     int64_t n, float inv_vs, double vs, int grad, float* out, ngs_stream s) {
+  if (!grids || !x || n_levels < 1 || n_levels > NGS_MAX_FIELD_LEVELS || n < 0 || (n > 0 && (!pos || !out)))
+    return NGS_ERR_INVALID_ARG;
+  FieldLevels fl;
+  fl.n = n_levels;
+  for (int l = 0; l < n_levels; l++) {
+    if (!grid_ok(grids[l]) || !x[l]) return NGS_ERR_INVALID_ARG;
+    fl.g[l] = grids[l];
+    fl.x[l] = x[l];
+  }
+  if (n == 0) return NGS_OK;
+  { ngs_count_launch(); eval_field_levels_kernel<<<ngs_blocks(n, 128), 128, 0, (cudaStream_t)s>>>(fl, pos, n, inv_vs, vs, grad, out); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
 }
 
 extern "C" int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv_vs, double vs, const float* x,

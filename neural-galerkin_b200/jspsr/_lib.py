@@ -20,6 +20,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "buffer or workspace too small", 3:
           4: "not converged", 5: "topology error", 6: "CUDA error", 7: "device-side wait timed out"}
 NGS_OK, NGS_ERR_INVALID_ARG, NGS_ERR_NOT_CONVERGED, NGS_ERR_TIMEOUT = 0, 1, 4, 7
 PCG_REFERENCE, PCG_MIXED, PCG_FP64 = 0, 1, 2
+MAX_FIELD_LEVELS = 16
 
 vp, i32, i64, f32, f64, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_double, C.c_size_t
 
@@ -81,10 +82,12 @@ _SIGS = {
     "ngs_point_basis": ([G, vp, i64, f32, f64, vp, vp, vp], C.c_int),
     "ngs_point_field": ([vp, vp, i64, vp, vp, C.c_int, vp], C.c_int),
     "ngs_eval_field": ([G, vp, i64, f32, f64, vp, C.c_int, vp, vp], C.c_int),
+    "ngs_eval_field_levels": ([C.POINTER(Grid), C.POINTER(vp), C.c_int, vp, i64, f32, f64, C.c_int, vp, vp], C.c_int),
     "ngs_weighted_sum": ([vp, vp, i64, vp, vp], C.c_int),
     "ngs_stencil_count": ([G, vp, i64, vp, vp, vp], C.c_int),
     "ngs_stencil_fill": ([G, vp, i64, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "ngs_screen_gram": ([vp, vp, i64, vp, vp, vp, f64, vp, vp], C.c_int),
+    "ngs_screen_gram_grouped": ([vp, vp, i64, vp, vp, vp, vp, vp, f64, vp, vp], C.c_int),
     "ngs_screen_rhs": ([vp, vp, i64, vp, f64, vp, vp], C.c_int),
     "ngs_rhs_normals": ([G, vp, i64, vp, G, vp, i64, vp, vp, C.c_int, vp, vp], C.c_int),
     "ngs_correction_stiffness": ([vp, i64, C.c_int, G, vp, vp, vp, C.c_int, vp, vp], C.c_int),

@@ -260,8 +260,14 @@ class Reconstruction:
                    L.ptr(st125), L.ptr(lv.cols), L.ptr(lv.vals64), L.ptr(lv.diag_slot), st)
             if self.alpha > 0:
                 sf = 0.25 ** d
-                L.call("ngs_screen_gram", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(lv.masks),
-                       L.ptr(lv.rowptr), sf * self.alpha, L.ptr(lv.vals64), st)
+                # group the points by cell: one atomic per (cell, slot) instead of per point
+                present = lv.rows >= 0
+                first = present.to(torch.int8).argmax(1)
+                key = lv.rows.gather(1, first[:, None]).squeeze(1).long() * 27 + first
+                key = torch.where(present.any(1), key, torch.full_like(key, -1))
+                keys, order = torch.sort(key)
+                L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(order),
+                       L.ptr(keys), L.ptr(lv.masks), L.ptr(lv.rowptr), sf * self.alpha, L.ptr(lv.vals64), st)
             lv.vals32 = torch.empty(lv.nnz, dtype=torch.float32, device=self.dev)
             lv.inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
             L.call("ngs_finish_system", L.ptr(lv.vals64), lv.nnz, L.ptr(lv.diag_slot), lv.n, L.ptr(lv.vals32),
@@ -433,9 +439,12 @@ class Reconstruction:
         """Sum over levels of the interpolated field at positions (reconstructor.py:197-226)."""
         pos = pos.contiguous().float()
         out = torch.zeros((pos.shape[0], 3) if grad else pos.shape[0], dtype=torch.float32, device=self.dev)
-        for lv in self.levels:
-            L.call("ngs_eval_field", lv.grid, L.ptr(pos), pos.shape[0], np.float32(self.inv_vs), self.vs,
-                   L.ptr(lv.x32), int(grad), L.ptr(out), L.stream())
+        for l0 in range(0, len(self.levels), L.MAX_FIELD_LEVELS):
+            lvs = self.levels[l0:l0 + L.MAX_FIELD_LEVELS]
+            grids = (L.Grid * len(lvs))(*[lv.grid for lv in lvs])
+            xs = (L.C.c_void_p * len(lvs))(*[lv.x32.data_ptr() for lv in lvs])
+            L.call("ngs_eval_field_levels", grids, xs, len(lvs), L.ptr(pos), pos.shape[0], np.float32(self.inv_vs),
+                   self.vs, int(grad), L.ptr(out), L.stream())
         return out
 
     def mean_chi(self) -> torch.Tensor:
