@@ -24,19 +24,41 @@ NGS_DEV int popc_below(const uint4 m, int o) {
 }
 
 // ----------------------------------------------------------------------------- structure
+// One warp per row: lane l < 25 owns the stencil column (dx, dy) = (l / 5 - 2, l % 5 - 2) and its
+// five cells along z (offsets o = 5 l .. 5 l + 4 in lexicographic order), found with one or two
+// bitmap words; a warp scan of the lanes' counts gives every lane its first CSR slot, so the row's
+// entries are written by consecutive lanes.
+NGS_DEV void stencil_column(const ngs_grid& g, const int32_t* __restrict__ coords, int64_t i, int lane,
+                            int32_t (&r)[5]) {
+  const int cx = coords[i * 3], cy = coords[i * 3 + 1], cz = coords[i * 3 + 2];
+  if (lane < 25)
+    grid_rows_zrun<5>(g, cx + (lane / 5 - 2) * g.stride, cy + (lane % 5 - 2) * g.stride, cz - 2 * g.stride, r);
+  else
+    for (int t = 0; t < 5; t++) r[t] = -1;
+}
+
 __global__ void stencil_count_kernel(ngs_grid g, const int32_t* __restrict__ coords, int64_t V,
                                      uint4* __restrict__ masks, int64_t* __restrict__ counts) {
-  for (int64_t i = ngs_gtid(); i < V; i += ngs_gstride()) {
-    const int cx = coords[i * 3], cy = coords[i * 3 + 1], cz = coords[i * 3 + 2];
-    unsigned w[4] = {0u, 0u, 0u, 0u};
-    int o = 0;
-    for (int dx = -2; dx <= 2; dx++)
-      for (int dy = -2; dy <= 2; dy++)
-        for (int dz = -2; dz <= 2; dz++, o++) {
-          if (grid_row(g, cx + dx * g.stride, cy + dy * g.stride, cz + dz * g.stride) >= 0) w[o >> 5] |= 1u << (o & 31);
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ngs_gtid() >> 5; i < V; i += warps) {
+    int32_t r[5];
+    stencil_column(g, coords, i, lane, r);
+    unsigned bal[5];                                  // bal[t] bit l: cell t of lane l's column is present
+#pragma unroll
+    for (int t = 0; t < 5; t++) bal[t] = __ballot_sync(0xffffffffu, r[t] >= 0);
+    if (lane == 0) {
+      unsigned w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int l = 0; l < 25; l++)
+#pragma unroll
+        for (int t = 0; t < 5; t++) {
+          const int o = 5 * l + t;
+          w[o >> 5] |= ((bal[t] >> l) & 1u) << (o & 31);
         }
-    masks[i] = make_uint4(w[0], w[1], w[2], w[3]);
-    counts[i] = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+      masks[i] = make_uint4(w[0], w[1], w[2], w[3]);
+      counts[i] = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+    }
   }
 }
 
@@ -47,21 +69,30 @@ __global__ void stencil_fill_kernel(ngs_grid g, const int32_t* __restrict__ coor
   __shared__ double st[125];
   for (int t = threadIdx.x; t < 125; t += blockDim.x) st[t] = stencil[t];
   __syncthreads();
-  for (int64_t i = ngs_gtid(); i < V; i += ngs_gstride()) {
-    const int cx = coords[i * 3], cy = coords[i * 3 + 1], cz = coords[i * 3 + 2];
-    const uint4 m = masks[i];
-    const unsigned w[4] = {m.x, m.y, m.z, m.w};
-    int64_t slot = rowptr[i];
-    int o = 0;
-    for (int dx = -2; dx <= 2; dx++)
-      for (int dy = -2; dy <= 2; dy++)
-        for (int dz = -2; dz <= 2; dz++, o++) {
-          if (!((w[o >> 5] >> (o & 31)) & 1u)) continue;
-          cols[slot] = (int32_t)grid_row(g, cx + dx * g.stride, cy + dy * g.stride, cz + dz * g.stride);
-          vals[slot] = st[o];
-          if (o == 62) diag_slot[i] = slot;
-          slot++;
-        }
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ngs_gtid() >> 5; i < V; i += warps) {
+    int32_t r[5];
+    stencil_column(g, coords, i, lane, r);
+    int c = 0;
+#pragma unroll
+    for (int t = 0; t < 5; t++) c += r[t] >= 0 ? 1 : 0;
+    int pre = c;                                      // inclusive warp scan of the counts
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, pre, d);
+      if (lane >= d) pre += y;
+    }
+    int64_t slot = rowptr[i] + (pre - c);
+#pragma unroll
+    for (int t = 0; t < 5; t++) {
+      if (r[t] < 0) continue;
+      const int o = 5 * lane + t;
+      cols[slot] = r[t];
+      vals[slot] = st[o];
+      if (o == 62) diag_slot[i] = slot;
+      slot++;
+    }
   }
 }
 
@@ -69,7 +100,7 @@ extern "C" int ngs_stencil_count(ngs_grid g, const int32_t* coords, int64_t V, u
                                  ngs_stream s) {
   if (!g.words || V < 0 || (V > 0 && (!coords || !masks || !counts))) return NGS_ERR_INVALID_ARG;
   if (V == 0) return NGS_OK;
-  { ngs_count_launch(); stencil_count_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(g, coords, V, reinterpret_cast<uint4*>(masks),
+  { ngs_count_launch(); stencil_count_kernel<<<ngs_blocks(V * 32, 256), 256, 0, (cudaStream_t)s>>>(g, coords, V, reinterpret_cast<uint4*>(masks),
                                                                        counts); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
@@ -81,7 +112,7 @@ extern "C" int ngs_stencil_fill(ngs_grid g, const int32_t* coords, int64_t V, co
   if (!g.words || V < 0 || (V > 0 && (!coords || !masks || !rowptr || !stencil125 || !cols || !vals || !diag_slot)))
     return NGS_ERR_INVALID_ARG;
   if (V == 0) return NGS_OK;
-  { ngs_count_launch(); stencil_fill_kernel<<<ngs_blocks(V, 128), 128, 0, (cudaStream_t)s>>>(
+  { ngs_count_launch(); stencil_fill_kernel<<<ngs_blocks(V * 32, 256), 256, 0, (cudaStream_t)s>>>(
       g, coords, V, reinterpret_cast<const uint4*>(masks), rowptr, stencil125, cols, vals, diag_slot); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;

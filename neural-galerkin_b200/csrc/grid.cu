@@ -321,33 +321,6 @@ extern "C" int ngs_point_field(const int32_t* rows, const float* phi, int64_t n,
   return NGS_OK;
 }
 
-// Rows of the three cells (x, y, z + t * stride), t = 0, 1, 2, or -1 where absent: the three share
-// one or two bitmap words, loaded once each.
-NGS_DEV void grid_rows_z3(const ngs_grid& g, int x, int y, int z, int32_t (&r)[3]) {
-  r[0] = r[1] = r[2] = -1;
-  const int dx = x - g.origin[0], dy = y - g.origin[1], dz = z - g.origin[2];
-  if ((dx | dy) < 0) return;
-  const int i = dx >> g.log2_stride, j = dy >> g.log2_stride;
-  if (i >= g.dims[0] || j >= g.dims[1]) return;
-  const uint4* row = reinterpret_cast<const uint4*>(g.words) + ((int64_t)i * g.dims[1] + j) * g.zwords;
-  const int k0 = dz >> g.log2_stride;               // arithmetic shift: floor for cells below the box
-  int have = -1;
-  uint4 v = make_uint4(0, 0, 0, 0);
-#pragma unroll
-  for (int t = 0; t < 3; t++) {
-    const int k = k0 + t;
-    if (k < 0 || k >= g.dims[2]) continue;
-    const int w = k >> 6;
-    if (w != have) {
-      v = __ldg(row + w);
-      have = w;
-    }
-    const unsigned long long bits = (unsigned long long)v.z | ((unsigned long long)v.w << 32);
-    const int b = k & 63;
-    if ((bits >> b) & 1ull) r[t] = (int32_t)(v.x + (unsigned)__popcll(bits & ((1ull << b) - 1ull)));
-  }
-}
-
 // One level's field (or gradient) at a point: 27 basis functions around it (hashtree.py:157-192,
 // bezier_tensor.py:56-73: the gradient is per finest-voxel unit / stride).  All nine bitmap probes
 // are issued before the coefficient gathers.
@@ -368,7 +341,7 @@ NGS_DEV void level_field(const ngs_grid& g, const float* p, float inv_vs, double
   for (int kx = 0; kx < 3; kx++)
 #pragma unroll
     for (int ky = 0; ky < 3; ky++)
-      grid_rows_z3(g, nb.q[0] + (kx - 1) * g.stride, nb.q[1] + (ky - 1) * g.stride, nb.q[2] - g.stride, rows[kx][ky]);
+      grid_rows_zrun<3>(g, nb.q[0] + (kx - 1) * g.stride, nb.q[1] + (ky - 1) * g.stride, nb.q[2] - g.stride, rows[kx][ky]);
   float lv = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
 #pragma unroll
   for (int kx = 0; kx < 3; kx++)

@@ -36,6 +36,35 @@ NGS_DEV int64_t grid_row(const ngs_grid& g, int x, int y, int z) {
   return (int64_t)v.x + __popcll(bits & ((1ull << b) - 1ull));
 }
 
+// Rows of K consecutive cells along z, (x, y, z + t * stride) for t = 0 .. K-1, or -1 where absent.
+// The run covers at most two bitmap words; each is loaded once.
+template <int K>
+NGS_DEV void grid_rows_zrun(const ngs_grid& g, int x, int y, int z, int32_t (&r)[K]) {
+#pragma unroll
+  for (int t = 0; t < K; t++) r[t] = -1;
+  const int dx = x - g.origin[0], dy = y - g.origin[1], dz = z - g.origin[2];
+  if ((dx | dy) < 0) return;
+  const int i = dx >> g.log2_stride, j = dy >> g.log2_stride;
+  if (i >= g.dims[0] || j >= g.dims[1]) return;
+  const uint4* row = reinterpret_cast<const uint4*>(g.words) + ((int64_t)i * g.dims[1] + j) * g.zwords;
+  const int k0 = dz >> g.log2_stride;               // arithmetic shift: floor for cells below the box
+  int have = -1;
+  uint4 v = make_uint4(0, 0, 0, 0);
+#pragma unroll
+  for (int t = 0; t < K; t++) {
+    const int k = k0 + t;
+    if (k < 0 || k >= g.dims[2]) continue;
+    const int w = k >> 6;
+    if (w != have) {
+      v = __ldg(row + w);
+      have = w;
+    }
+    const unsigned long long bits = (unsigned long long)v.z | ((unsigned long long)v.w << 32);
+    const int b = k & 63;
+    if ((bits >> b) & 1ull) r[t] = (int32_t)(v.x + (unsigned)__popcll(bits & ((1ull << b) - 1ull)));
+  }
+}
+
 NGS_DEV int64_t grid_word_index(const ngs_grid& g, int x, int y, int z, int* bit) {
   const int dx = x - g.origin[0], dy = y - g.origin[1], dz = z - g.origin[2];
   if ((dx | dy | dz) < 0) return -1;

@@ -11,7 +11,7 @@
 //     barrier + reduce     the last block to arrive sums the per-block partials in
 //                          block order (deterministic) and releases the others.
 // The SpMV streams the CSR arrays straight from HBM: eight lanes per row, each lane
-// with four (column, value) pairs and their vector gathers in flight per round, at
+// with up to eight (column, value) pairs and their vector gathers in flight per round, at
 // two blocks per SM.  (Staging CSR tiles through shared memory with bulk copies ran at
 // less than half this rate: the product and row-sum passes over shared memory, not
 // the copies, bounded it.)
@@ -136,16 +136,24 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
     const int64_t e0 = a.rowptr[row], e1 = a.rowptr[row + 1];
     const double2 ax = pre(row);
     ACC acc = (ACC)0;
-    int64_t j = e0 + sub;
-    for (; j + 3 * L < e1; j += 4 * L) {
-      const int32_t c0 = ld_stream(a.cols + j), c1 = ld_stream(a.cols + j + L);
-      const int32_t c2 = ld_stream(a.cols + j + 2 * L), c3 = ld_stream(a.cols + j + 3 * L);
-      const MT m0 = ld_stream(vals + j), m1 = ld_stream(vals + j + L);
-      const MT m2 = ld_stream(vals + j + 2 * L), m3 = ld_stream(vals + j + 3 * L);
-      const VT x0 = v[c0], x1 = v[c1], x2 = v[c2], x3 = v[c3];
-      acc += (ACC)m0 * (ACC)x0 + (ACC)m1 * (ACC)x1 + (ACC)m2 * (ACC)x2 + (ACC)m3 * (ACC)x3;
+    // rounds of U entries per lane, predicated: a 5x5x5 stencil row (<= 125 entries, ~60 on a
+    // surface) takes one or two rounds, with all of a round's loads and gathers in flight
+    constexpr int U = 8;
+    for (int64_t j0 = e0 + sub; j0 < e1; j0 += U * L) {
+      int32_t c[U];
+      MT m[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        const int64_t j = j0 + (int64_t)k * L;
+        c[k] = j < e1 ? ld_stream(a.cols + j) : -1;
+        m[k] = j < e1 ? ld_stream(vals + j) : (MT)0;
+      }
+      VT xv[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) xv[k] = c[k] >= 0 ? v[c[k]] : (VT)0;
+#pragma unroll
+      for (int k = 0; k < U; k++) acc += (ACC)m[k] * (ACC)xv[k];
     }
-    for (; j < e1; j += L) acc += (ACC)ld_stream(vals + j) * (ACC)v[ld_stream(a.cols + j)];
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
     if (sub == 0) dsum += epi(row, (double)acc, ax);

@@ -442,6 +442,48 @@ def learned_case():
     print("learned", float(loss), {k: v.shape for k, v in out.items() if k.startswith(("coords", "grad"))})
 
 
+def _count_policy(xyz, inds, min_count=6):
+    """Test subdivision policy: keep subdividing the cells that hold at least min_count points."""
+    counts = torch.bincount(inds)
+    return counts[inds] >= min_count
+
+
+def structure_case():
+    """The hierarchy builders and queries beside the density-adaptive one (``hashtree.py:240-312``,
+    ``_hash_backend.py:292-412``): dense hierarchy, subdivision by a policy, voxel status,
+    expanded / conforming coordinates, test grid and trilinear split of voxel data."""
+    from jspsr.core.hashtree import HashTree
+    xyz, nrm = synthetic.torus(n=3000, seed=1)
+    xyz_t = torch.from_numpy(xyz)
+    out = dict(xyz=xyz)
+    dense = HashTree(xyz_t, voxel_size=1.0 / 64, depth=3)
+    dense.build_encoder_hierarchy_dense(expand_range=3)
+    dense.reflect_decoder_coords()
+    out["dense_density"] = dense.xyz_density.numpy()
+    rng = np.random.default_rng(5)
+    for d in range(3):
+        c = dense.get_coords(dense.ENCODER, d)
+        out[f"dense{d}"] = c.numpy()
+        s = dense.get_stride(dense.ENCODER, d)
+        probe = torch.cat([c[::7], c[::11] + s, torch.from_numpy(rng.integers(-40, 40, (64, 3)).astype(np.int32)) * s])
+        out[f"probe{d}"] = probe.numpy()
+        out[f"status{d}"] = dense.evaluate_voxel_status(dense.ENCODER, probe, d).numpy()
+        out[f"expand{d}"] = dense._enc_branch.get_coords(d, expand=3).numpy()
+        out[f"conform{d}"] = dense._enc_branch.get_coords(d, conforming=True).numpy()
+        data = torch.from_numpy(rng.normal(size=(c.shape[0], 2)).astype(np.float32))
+        out[f"data{d}"] = data.numpy()
+        out[f"split{d}"] = dense.split_data(xyz_t, dense.ENCODER, d, data).numpy()
+    q, base = dense.get_test_grid(3, 1, expand=0, conforming=False)
+    out["test_grid_pos"], out["test_grid_base"] = q.numpy(), base.numpy()
+    sub = HashTree(xyz_t, voxel_size=1.0 / 64, depth=3)
+    sub.build_hierarchy_subdivide(_count_policy, expand=True, min_count=6)
+    out["sub_depth"] = sub.xyz_depth.numpy()
+    for d in range(3):
+        out[f"sub{d}"] = sub.get_coords(sub.ENCODER, d).numpy()
+    np.savez_compressed(HERE / "structure.npz", **out)
+    print("structure", {k: v.shape for k, v in out.items() if k.startswith(("dense", "sub", "status"))})
+
+
 def main():
     _prepare_reference()
     names = sys.argv[1:]
@@ -449,6 +491,8 @@ def main():
         tables_case()
         mc_tables_case()
         range_kernel_case()
+    if not names or "structure" in names:
+        structure_case()
     if not names or "learned" in names:
         additive_tables_case()
         learned_case()
