@@ -75,6 +75,7 @@ struct PcgArgs {
   unsigned long long* deadline;   // absolute global-timer deadline, set at the first reduction
   unsigned long long budget_ns;   // time budget of the whole solve
   unsigned int nblocks;
+  int evict_first;                // stream the matrix past the caches (it does not fit L2)
 };
 
 constexpr int NGS_PCG_ITER_CAP = 20000;
@@ -117,9 +118,10 @@ NGS_DEV bool block_rows(const PcgArgs& a, unsigned bid, int64_t& row0, int64_t& 
   return __syncthreads_or(bad) == 0;
 }
 
-// Streaming loads of the (immutable) matrix: read-only path, no L1 allocation.
+// Loads of the (immutable) matrix.  A matrix larger than L2 is streamed evict-first, so that the
+// gathered vector keeps its place in the caches; a smaller one stays cached for the next iteration.
 template <typename T>
-NGS_DEV T ld_stream(const T* p) { return __ldg(p); }
+NGS_DEV T ld_mat(const T* p, bool stream) { return stream ? __ldcs(p) : __ldg(p); }
 
 // y = A v over rows [row0, row1): eight lanes per row.  epi(row, acc, pre(row)) consumes each
 // row's product (lane 0 of its group) and returns a contribution to the thread's partial sum.
@@ -145,8 +147,8 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
 #pragma unroll
       for (int k = 0; k < U; k++) {
         const int64_t j = j0 + (int64_t)k * L;
-        c[k] = j < e1 ? ld_stream(a.cols + j) : -1;
-        m[k] = j < e1 ? ld_stream(vals + j) : (MT)0;
+        c[k] = j < e1 ? ld_mat(a.cols + j, a.evict_first) : -1;
+        m[k] = j < e1 ? ld_mat(vals + j, a.evict_first) : (MT)0;
       }
       VT xv[U];
 #pragma unroll
@@ -718,6 +720,8 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.wait_ns = (unsigned long long)(timeout * 1e9);
   a.budget_ns = a.wait_ns;
   a.inner_rtol = 1.0e-4;
+  const size_t mat_bytes = (size_t)sys->nnz * (4 + (mode == NGS_PCG_FP64 ? 8 : 4));
+  a.evict_first = mat_bytes > (size_t)96 << 20;
   return NGS_OK;
 }
 
