@@ -395,6 +395,7 @@ def main():
     # ---------------------------------------------------------------- comparators: plain FP64 GPU and FP64 field error
     extra = {}
     if not args.no_comparators:
+        step(solver=PLAIN_SOLVER)        # warm-up: the comparator's kernels load on first use
         torch.cuda.synchronize()
         c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         c0.record()
