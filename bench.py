@@ -407,6 +407,7 @@ def main():
         plain_rec, _, _ = step(solver=PLAIN_SOLVER, profile=True)
         plain_solve = plain_rec.pcg_ms
         plain_iters = {d: int(lv.info[0]) for d, lv in enumerate(plain_rec.levels)}
+        step(solver=FP64_SOLVER)         # warm-up of the FP64 kernel, as above
         ref64, _, _ = step(solver=FP64_SOLVER, profile=True)
         fp64_solve = ref64.pcg_ms
         chi = rec.chi_raw(X) - rec.mean_chi()
