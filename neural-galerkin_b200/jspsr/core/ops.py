@@ -62,12 +62,15 @@ class MarchingCubes(torch.autograd.Function):
     def forward(ctx, base_coords, sdf_val, bandwidth=1.0):
         tris, vert_ids, src_ids, src_w = ext.marching_cubes_sparse(base_coords, sdf_val)
         unq, tri_idx = torch.unique(vert_ids.view(-1, 4), dim=0, return_inverse=True)
-        vertices = torch.empty((unq.size(0), 3), device=vert_ids.device)
-        vertices[tri_idx] = tris.view(-1, 3)
-        vsrc = torch.empty((unq.size(0), 2), dtype=src_ids.dtype, device=src_ids.device)
-        vsrc[tri_idx] = src_ids.view(-1, 2)
-        vw = torch.empty((unq.size(0), 1), dtype=src_w.dtype, device=src_w.device)
-        vw[tri_idx] = src_w.view(-1, 1)
+        # each vertex takes the edge data of its first occurrence, whole: the occurrences of an edge
+        # may list its two grid samples in either order (with w and 1 - w), so mixing columns of
+        # different occurrences would pair a sample with the other one's weight
+        n_occ = tri_idx.numel()
+        first = torch.full((unq.size(0),), n_occ, dtype=torch.int64, device=vert_ids.device)
+        first.scatter_reduce_(0, tri_idx, torch.arange(n_occ, device=vert_ids.device), reduce="amin")
+        vertices = tris.view(-1, 3)[first].float()
+        vsrc = src_ids.view(-1, 2)[first]
+        vw = src_w.view(-1, 1)[first]
         triangles = tri_idx.view(-1, 3)
         normals = compute_normal(vertices, triangles)
         ctx.save_for_backward(normals, vsrc.long(), vw)

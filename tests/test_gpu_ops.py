@@ -181,6 +181,69 @@ def test_primal_marching_cubes():
     np.testing.assert_allclose(sw, rw, atol=1e-5)
 
 
+def _mc_autograd_oracle(base, sdf, grad_vert, bandwidth):
+    """numpy restatement of the differentiable primal MC (``ops.py:9-58``): vertices deduplicated by
+    their edge ids, area-weighted normals, and the backward that hands each vertex's normal
+    component of grad_vert to the two grid values of its edge."""
+    tris, vids, sids, sw = O.marching_cubes_sparse(base, sdf)
+    unq, inv = np.unique(vids.reshape(-1, 4), axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    verts = np.zeros((unq.shape[0], 3), np.float64)
+    verts[inv] = tris.reshape(-1, 3)
+    vsrc = np.zeros((unq.shape[0], 2), np.int64)
+    vsrc[inv] = sids.reshape(-1, 2)
+    vw = np.zeros(unq.shape[0], np.float64)
+    vw[inv] = sw.reshape(-1)
+    faces = inv.reshape(-1, 3)
+    e1 = verts[faces[:, 1]] - verts[faces[:, 0]]
+    e2 = verts[faces[:, 2]] - verts[faces[:, 0]]
+    fn = np.cross(e1, e2)
+    vn = np.zeros_like(verts)
+    for k in range(3):
+        np.add.at(vn, faces[:, k], fn)
+    vn /= np.linalg.norm(vn, axis=1, keepdims=True) + 1e-6
+    g = bandwidth * (grad_vert[: verts.shape[0]] * vn).sum(1)
+    grid = np.zeros(sdf.size)
+    np.add.at(grid, vsrc[:, 0], vw * g)
+    np.add.at(grid, vsrc[:, 1], (1 - vw) * g)
+    return verts, faces, vn, grid.reshape(sdf.shape)
+
+
+def test_marching_cubes_autograd():
+    """``MarchingCubes`` (vertices, triangles, normals, and the backward to the grid values) against
+    its numpy restatement over the oracle's primal MC."""
+    from jspsr.core.ops import marching_cubes_op
+    M, r = 30, 4
+    g = np.stack(np.meshgrid(*[np.arange(r + 1)] * 3, indexing="ij"), -1).astype(np.float32)
+    base = np.array([[i, j, k] for i in range(-2, 1) for j in range(-2, 1) for k in range(-2, 1)][:M], np.float32)
+    base = base[: min(M, base.shape[0])]
+    pts = base[:, None, None, None, :] + g[None] / r
+    sdf = (np.linalg.norm(pts + 0.1, axis=-1) - 1.3).astype(np.float32)       # a sphere through the blocks
+    sdf_t = t(sdf).requires_grad_(True)
+    v, f, n, _ = marching_cubes_op(t(base), sdf_t, 1.0)
+    rng = np.random.default_rng(3)
+    gv = rng.normal(size=(v.shape[0], 3)).astype(np.float32)
+    (v * t(gv)).sum().backward()
+    rv, rf, rn, rg = _mc_autograd_oracle(base, sdf, gv, 1.0)
+    np.testing.assert_array_equal(f.cpu().numpy(), rf)
+    np.testing.assert_allclose(v.detach().cpu().numpy(), rv, atol=1e-5)
+    np.testing.assert_allclose(n.detach().cpu().numpy(), rn, atol=1e-4)
+    # an edge on a block boundary is seen from both blocks, each with its own copy of the boundary
+    # samples, and which copy its vertex draws from is arbitrary (the reference's "randomly pick one
+    # solution for overlapping edges"): compare the gradients summed per lattice position
+    loc = np.stack(np.meshgrid(*[np.arange(r + 1)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    lattice = (base.astype(np.int64)[:, None, :] * r + loc[None]).reshape(-1, 3)
+    keys, inv = np.unique(lattice, axis=0, return_inverse=True)
+
+    def per_position(gr):
+        out = np.zeros(keys.shape[0])
+        np.add.at(out, inv.reshape(-1), gr.reshape(-1))
+        return out
+    got = per_position(sdf_t.grad.cpu().numpy().astype(np.float64))
+    ref = per_position(rg)
+    assert np.linalg.norm(got - ref) <= 1e-4 * np.linalg.norm(ref)
+
+
 def test_dual_marching_cubes_ops(golden):
     """Dual-grid accumulation and dual MC on the oracle's structures and values (sign pattern given)."""
     from jspsr import ext
