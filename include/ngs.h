@@ -156,6 +156,12 @@ int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv_vs, double
 #define NGS_MAX_FIELD_LEVELS 16
 int ngs_eval_field_levels(const ngs_grid* grids, const float* const* x, int n_levels, const float* pos, int64_t n,
                           float inv_vs, double vs, int grad, float* out, ngs_stream s);
+/* The field (grad 0) at the 2x2x2 mesh samples of n_cells leaf cells of level cell_level (pos and out:
+ * 8 samples per cell, (ex, ey, ez) lexicographic, as ngs_expand_cells writes them with n_up = 2):
+ * the samples of a cell share the 4x4x4 neighbourhood of every level at least as coarse as the cell.
+ * Same sums as ngs_eval_field_levels on those positions, accumulated into out. */
+int ngs_eval_field_cells(const ngs_grid* grids, const float* const* x, int n_levels, int64_t n_cells, int cell_level,
+                         const float* pos, float inv_vs, double vs, float* out, ngs_stream s);
 /* sum_p w[p] * v[p] and sum_p w[p] into sums_dev double[2] (mean-chi level set). */
 int ngs_weighted_sum(const float* v, const float* w, int64_t n, double* sums_dev, ngs_stream s);
 

@@ -207,17 +207,21 @@ struct PointNbr {
   float rel[3][3];
 };
 
+// One axis of a point's neighbourhood: the cell q the point falls in and the basis arguments of the
+// cells q - stride, q, q + stride.
+NGS_DEV void axis_nbr(float p, float inv_vs, double vs, int stride, float inv_s, int& q, float (&rel)[3]) {
+  q = point_quant(q32(p, inv_vs), stride, inv_s);
+  const double pos = (double)p / vs - 0.5;
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    rel[k] = (float)((pos - (double)q - (double)((k - 1) * stride) - 0.5 * (stride - 1)) / stride);
+}
+
 NGS_DEV PointNbr point_nbr(const float* p, float inv_vs, double vs, int stride) {
   PointNbr r;
   const float inv_s = 1.0f / (float)stride;
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
-    r.q[a] = point_quant(q32(p[a], inv_vs), stride, inv_s);
-    const double pos = (double)p[a] / vs - 0.5;
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-      r.rel[a][k] = (float)((pos - (double)r.q[a] - (double)((k - 1) * stride) - 0.5 * (stride - 1)) / stride);
-  }
+  for (int a = 0; a < 3; a++) axis_nbr(p[a], inv_vs, vs, stride, inv_s, r.q[a], r.rel[a]);
   return r;
 }
 
@@ -417,6 +421,101 @@ __global__ void __launch_bounds__(128, 6) eval_field_levels_kernel(const __grid_
       out[p * 3 + 2] = sz;
     }
   }
+}
+
+// The field at the 2 x 2 x 2 mesh samples of leaf cells (the primal samples of the dual marching
+// cubes, n_upsample = 2): pos holds the 8 samples of cell c at 8c .. 8c+7, (ex, ey, ez) in
+// lexicographic order, and along each axis they take two positions.  On a field level at least as
+// coarse as the cells, the 8 samples' 27-cell neighbourhoods lie in one 4 x 4 x 4 box: the box is
+// looked up once (16 runs of 4 cells along z) into shared memory and every sample sums its 27
+// terms from there, in the same order and with the same basis values as eval_field_levels.  Finer
+// field levels take the per-sample path.  Levels are added in level order.
+__global__ void __launch_bounds__(128) field_cells_kernel(const __grid_constant__ FieldLevels fl,
+                                                          int64_t n_cells, int cell_level, const float* __restrict__ pos,
+                                                          float inv_vs, double vs, float* __restrict__ out) {
+  // box entry i of thread t at boxes[i][t]: the threads of a warp touch consecutive banks
+  __shared__ float boxes[64][128];
+  float* box = &boxes[0][threadIdx.x];
+  for (int64_t c = ngs_gtid(); c < n_cells; c += ngs_gstride()) {
+    const float* P = pos + c * 24;
+    float acc[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) acc[e] = out[c * 8 + e];
+    for (int l = 0; l < fl.n; l++) {
+      const ngs_grid& g = fl.g[l];
+      const float* __restrict__ x = fl.x[l];
+      const int S = g.stride;
+      const float inv_s = 1.0f / (float)S;
+      // per axis a and side t: the samples' cell and basis values (sample (t,0,0) carries x, ...)
+      int q[3][2];
+      float b[3][2][3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          float rel[3];
+          axis_nbr(P[(t << (2 - a)) * 3 + a], inv_vs, vs, S, inv_s, q[a][t], rel);
+#pragma unroll
+          for (int k = 0; k < 3; k++) b[a][t][k] = bspline(rel[k]);
+        }
+      const bool boxed = l >= cell_level && q[0][1] - q[0][0] <= S && q[1][1] - q[1][0] <= S &&
+                         q[2][1] - q[2][0] <= S && q[0][1] >= q[0][0] && q[1][1] >= q[1][0] && q[2][1] >= q[2][0];
+      if (!boxed) {
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+          float v, gx, gy, gz;
+          level_field(g, P + e * 3, inv_vs, vs, x, 0, v, gx, gy, gz);
+          acc[e] += v;
+        }
+        continue;
+      }
+      const int ox = q[0][0] - S, oy = q[1][0] - S, oz = q[2][0] - S;
+#pragma unroll
+      for (int ix = 0; ix < 4; ix++)
+#pragma unroll
+        for (int iy = 0; iy < 4; iy++) {
+          int32_t r[4];
+          grid_rows_zrun<4>(g, ox + ix * S, oy + iy * S, oz, r);
+#pragma unroll
+          for (int iz = 0; iz < 4; iz++) box[((ix * 4 + iy) * 4 + iz) * 128] = r[iz] >= 0 ? x[r[iz]] : 0.f;
+        }
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int tx = e >> 2, ty = (e >> 1) & 1, tz = e & 1;
+        const int bx = (q[0][tx] - q[0][0]) / S, by = (q[1][ty] - q[1][0]) / S, bz = (q[2][tz] - q[2][0]) / S;
+        float lv = 0.f;
+#pragma unroll
+        for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+          for (int ky = 0; ky < 3; ky++)
+#pragma unroll
+            for (int kz = 0; kz < 3; kz++)
+              lv += b[0][tx][kx] * b[1][ty][ky] * b[2][tz][kz] * box[(((bx + kx) * 4 + (by + ky)) * 4 + (bz + kz)) * 128];
+        acc[e] += lv;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 8; e++) out[c * 8 + e] = acc[e];
+  }
+}
+
+extern "C" int ngs_eval_field_cells(const ngs_grid* grids, const float* const* x, int n_levels, int64_t n_cells,
+                                    int cell_level, const float* pos, float inv_vs, double vs, float* out,
+                                    ngs_stream s) {
+  if (!grids || !x || n_levels < 1 || n_levels > NGS_MAX_FIELD_LEVELS || n_cells < 0 ||
+      (n_cells > 0 && (!pos || !out)))
+    return NGS_ERR_INVALID_ARG;
+  FieldLevels fl;
+  fl.n = n_levels;
+  for (int l = 0; l < n_levels; l++) {
+    if (!grid_ok(grids[l]) || !x[l]) return NGS_ERR_INVALID_ARG;
+    fl.g[l] = grids[l];
+    fl.x[l] = x[l];
+  }
+  if (n_cells == 0) return NGS_OK;
+  { ngs_count_launch(); field_cells_kernel<<<ngs_blocks(n_cells, 128), 128, 0, (cudaStream_t)s>>>(fl, n_cells, cell_level, pos, inv_vs, vs, out); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
 }
 
 extern "C" int ngs_eval_field_levels(const ngs_grid* grids, const float* const* x, int n_levels, const float* pos,

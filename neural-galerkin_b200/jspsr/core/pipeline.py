@@ -447,6 +447,24 @@ class Reconstruction:
                    self.vs, int(grad), L.ptr(out), L.stream())
         return out
 
+    def chi_cells(self, pos: torch.Tensor, starts, counts) -> torch.Tensor:
+        """chi_raw at the 2x2x2 samples of the leaf cells, level by level: segment d of pos (starts[d],
+        counts[d] samples) holds the samples of level-d cells, 8 per cell in expansion order.  The
+        samples of one cell share the neighbourhood of every coarser field level, which is read once
+        per cell."""
+        out = torch.zeros(pos.shape[0], dtype=torch.float32, device=self.dev)
+        for d, cnt in enumerate(counts):
+            if cnt == 0:
+                continue
+            seg = slice(int(starts[d]), int(starts[d]) + cnt)
+            for l0 in range(0, len(self.levels), L.MAX_FIELD_LEVELS):
+                lvs = self.levels[l0:l0 + L.MAX_FIELD_LEVELS]
+                grids = (L.Grid * len(lvs))(*[lv.grid for lv in lvs])
+                xs = (L.C.c_void_p * len(lvs))(*[lv.x32.data_ptr() for lv in lvs])
+                L.call("ngs_eval_field_cells", grids, xs, len(lvs), cnt // 8, d - l0, L.ptr(pos[seg]),
+                       np.float32(self.inv_vs), self.vs, L.ptr(out[seg]), L.stream())
+        return out
+
     def mean_chi(self) -> torch.Tensor:
         """Density-weighted mean of chi at the input points (reconstructor.py:228-236), as a device scalar."""
         chi = torch.zeros(self.n, dtype=torch.float32, device=self.dev)
@@ -563,7 +581,7 @@ class Reconstruction:
         self.topology_overflow = cnt  # counts above 8 mark the reference's "Topology Error"
         self._mark("dual grid")
         # field at the primal samples
-        vals = self.chi_raw(pos) - mean
+        vals = (self.chi_cells(pos, starts, counts) if n_upsample == 2 else self.chi_raw(pos)) - mean
         self._mark("chi")
         # marching cubes
         vcount = torch.empty(m, dtype=torch.int32, device=dev)

@@ -108,6 +108,19 @@ def test_dual_grid_bit_exact(cases, gpu_runs, name):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_cell_field_matches_point_field(gpu_runs, name):
+    """The per-cell evaluation of the mesh samples (one neighbourhood read per cell and coarser
+    level) sums the same terms as the per-sample evaluation: equal up to FP32 contraction order."""
+    rec = gpu_runs[name][0]
+    info = rec.mesh_info
+    counts = info["counts"]
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    cells = rec.chi_cells(info["positions"], starts, counts).cpu().numpy()
+    points = rec.chi_raw(info["positions"]).cpu().numpy()
+    assert np.abs(cells - points).max() <= 1e-6 * max(np.abs(points).max(), 1e-30)
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_mesh_matches_oracle(cases, gpu_runs, name):
     g, _, mesh = cases[name]
     rec, v, f = gpu_runs[name]
