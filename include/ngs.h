@@ -156,11 +156,12 @@ int ngs_eval_field(ngs_grid g, const float* pos, int64_t n, float inv_vs, double
 #define NGS_MAX_FIELD_LEVELS 16
 int ngs_eval_field_levels(const ngs_grid* grids, const float* const* x, int n_levels, const float* pos, int64_t n,
                           float inv_vs, double vs, int grad, float* out, ngs_stream s);
-/* The field (grad 0) at the 2x2x2 mesh samples of n_cells leaf cells of level cell_level (pos and out:
- * 8 samples per cell, (ex, ey, ez) lexicographic, as ngs_expand_cells writes them with n_up = 2):
- * the samples of a cell share the 4x4x4 neighbourhood of every level at least as coarse as the cell.
- * Same sums as ngs_eval_field_levels on those positions, accumulated into out. */
-int ngs_eval_field_cells(const ngs_grid* grids, const float* const* x, int n_levels, int64_t n_cells, int cell_level,
+/* The field (grad 0) at the 2x2x2 mesh samples of n_cells leaf cells (pos and out: 8 samples per cell,
+ * (ex, ey, ez) lexicographic, as ngs_expand_cells writes them with n_up = 2).  On every level whose
+ * cells are at least half the leaf cell's size, the samples of a cell share one 4x4x4 neighbourhood,
+ * read once.  Same sums as ngs_eval_field_levels on those positions (contracted axis by axis),
+ * accumulated into out. */
+int ngs_eval_field_cells(const ngs_grid* grids, const float* const* x, int n_levels, int64_t n_cells,
                          const float* pos, float inv_vs, double vs, float* out, ngs_stream s);
 /* sum_p w[p] * v[p] and sum_p w[p] into sums_dev double[2] (mean-chi level set). */
 int ngs_weighted_sum(const float* v, const float* w, int64_t n, double* sums_dev, ngs_stream s);
@@ -341,8 +342,12 @@ int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_t* primal_b
 int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, ngs_stream s);
 int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, const int64_t* keep_offset, int64_t n,
                         int32_t* acc_out, ngs_stream s);
-int ngs_dual_mc_count(const int32_t* acc, int64_t n_cubes, const float* values, int32_t* vcount, ngs_stream s);
-int ngs_dual_mc_emit(const int32_t* acc, int64_t n_cubes, const float* pos, const float* values,
+/* Dual MC over n_cubes cubes of acc.  cnt (nullable): the accumulation counts of an uncompacted acc;
+ * cubes whose count is not 8 emit nothing, so the triangles come out as from the compacted acc and
+ * the select / compact pass can be skipped.  NULL: every cube is complete (the reference's op). */
+int ngs_dual_mc_count(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* values, int32_t* vcount,
+                      ngs_stream s);
+int ngs_dual_mc_emit(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* pos, const float* values,
                      const int64_t* voffset, float* tris, int32_t* vert_ids, ngs_stream s);
 /* Vertex de-duplication of (vid0, vid1) edge keys (replaces torch.unique(dim=0, return_inverse),
  * ref: jspsr/core/reconstructor.py:380-383): bucket sort by vid0 over n_primal buckets.

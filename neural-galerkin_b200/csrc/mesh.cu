@@ -43,70 +43,102 @@ NGS_DEV float sdf_interp(const float* p1, const float* p2, float v1, float v2, f
 }
 
 // ----------------------------------------------------------------------------- dual corner accumulation
-template <typename Lookup>
-__global__ void dual_inds_kernel(Lookup lk, const int32_t* __restrict__ pb, int64_t n_primal, int stride, int depth,
+// The probes of one primal cell of stride s: its 8 corners (one dual-cube slot each), the 12 (s - 1)
+// interior points of its edges (two slots) and the 6 (s - 1)^2 interior points of its faces (four
+// slots).  The index space is laid out kind by kind -- all corner probes, then all edge probes,
+// then all face probes -- so that the threads of a warp take the same branch, and it is indexed in
+// 32 bits whenever it fits.
+//
+// More than 8 slot writes into one dual cube is the reference's "Topology Error"
+// (dual_mc_inds.cu:86,115,135): such a cube's count ends above 8 and the cube is dropped by
+// ngs_dual_mc_select, which keeps the cubes with exactly 8 writes; every probe therefore writes its
+// slots unconditionally and adds to the count without reading it back.
+template <typename Lookup, typename Idx>
+__global__ void dual_inds_kernel(Lookup lk, const int32_t* __restrict__ pb, Idx n_primal, int stride, int depth,
                                  int64_t idx_base, int32_t* __restrict__ acc, int32_t* __restrict__ cnt) {
-  const int sm1 = stride - 1;
-  const int64_t per = 8 + 12 * (int64_t)sm1 + 6 * (int64_t)sm1 * sm1;
-  const int64_t total = n_primal * per;
-  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
-    const int64_t pid = t / per;
-    int64_t q = t - pid * per;
-    int off[3];
-    int slots[4], ns;
-    if (q < 8) {
+  const Idx sm1 = (Idx)stride - 1;
+  const Idx n_corner = n_primal * 8, n_edge = n_primal * 12 * sm1;
+  const Idx total = n_corner + n_edge + n_primal * 6 * sm1 * sm1;
+  for (Idx t = (Idx)ngs_gtid(); t < total; t += (Idx)ngs_gstride()) {
+    Idx pid;
+    // the probe's offset from the cell's base corner and its slots, kept in registers (axes are
+    // chosen with selects, not by indexing)
+    int off[3] = {0, 0, 0};
+    auto put = [&](int axis, int v) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) off[k] = axis == k ? v : off[k];
+    };
+    int slots[4] = {0, 0, 0, 0}, ns;
+    if (t < n_corner) {
+      pid = t >> 3;
+      const int q = (int)(t & 7);
       // corner (cx, cy, cz) = bits of q (x most significant): primal in the opposite octant
-      const int c[3] = {(int)(q >> 2) & 1, (int)(q >> 1) & 1, (int)q & 1};
-      for (int a = 0; a < 3; a++) off[a] = c[a] * stride;
-      slots[0] = c_octant_slot[(1 - c[0]) + 2 * (1 - c[1]) + 4 * (1 - c[2])];
+      const int cx = (q >> 2) & 1, cy = (q >> 1) & 1, cz = q & 1;
+      off[0] = cx * stride;
+      off[1] = cy * stride;
+      off[2] = cz * stride;
+      slots[0] = c_octant_slot[(1 - cx) + 2 * (1 - cy) + 4 * (1 - cz)];
       ns = 1;
-    } else if (q < 8 + 12 * (int64_t)sm1) {
-      q -= 8;
-      const int e = (int)(q / sm1), tt = (int)(q % sm1) + 1;
+    } else if (t < n_corner + n_edge) {
+      const Idx q = t - n_corner, per = 12 * sm1;
+      pid = q / per;
+      const Idx in = q - pid * per;
+      const int e = (int)(in / sm1), tt = (int)(in - (Idx)e * sm1) + 1;
       const int ax = e >> 2, v0 = (e >> 1) & 1, v1 = e & 1;
       const int b0 = ax == 0 ? 1 : 0, b1 = ax == 2 ? 1 : 2;
-      off[ax] = tt;
-      off[b0] = v0 * stride;
-      off[b1] = v1 * stride;
-      for (int o = 0; o < 2; o++) {
-        int oc[3];
-        oc[ax] = o;
-        oc[b0] = 1 - v0;
-        oc[b1] = 1 - v1;
-        slots[o] = c_octant_slot[oc[0] + 2 * oc[1] + 4 * oc[2]];
-      }
+      put(ax, tt);
+      put(b0, v0 * stride);
+      put(b1, v1 * stride);
+      // octant (oc[ax] = o, oc[b0] = 1 - v0, oc[b1] = 1 - v1) as ox + 2 oy + 4 oz
+      const int rest = ((1 - v0) << b0) + ((1 - v1) << b1);
+      slots[0] = c_octant_slot[rest];
+      slots[1] = c_octant_slot[rest + (1 << ax)];
       ns = 2;
     } else {
-      q -= 8 + 12 * (int64_t)sm1;
-      const int64_t fc = (int64_t)sm1 * sm1;
-      const int f = (int)(q / fc);
-      const int64_t in = q % fc;
+      const Idx q = t - n_corner - n_edge, fc = sm1 * sm1, per = 6 * fc;
+      pid = q / per;
+      const Idx in = q - pid * per;
+      const int f = (int)(in / fc);
+      const int uv = (int)(in - (Idx)f * fc);
       const int ax = f >> 1, side = f & 1;
       const int b0 = ax == 0 ? 1 : 0, b1 = ax == 2 ? 1 : 2;
-      off[ax] = side * stride;
-      off[b0] = (int)(in % sm1) + 1;
-      off[b1] = (int)(in / sm1) + 1;
-      for (int o = 0; o < 4; o++) {
-        int oc[3];
-        oc[ax] = 1 - side;
-        oc[b0] = o & 1;
-        oc[b1] = o >> 1;
-        slots[o] = c_octant_slot[oc[0] + 2 * oc[1] + 4 * oc[2]];
-      }
+      put(ax, side * stride);
+      put(b0, uv % (int)sm1 + 1);
+      put(b1, uv / (int)sm1 + 1);
+      // octant (oc[ax] = 1 - side, oc[b0] = o & 1, oc[b1] = o >> 1)
+      const int base = (1 - side) << ax;
+#pragma unroll
+      for (int o = 0; o < 4; o++) slots[o] = c_octant_slot[base + ((o & 1) << b0) + ((o >> 1) << b1)];
       ns = 4;
     }
-    const int64_t row = lk(pb[pid * 3] + off[0], pb[pid * 3 + 1] + off[1], pb[pid * 3 + 2] + off[2]);
+    const int64_t row = lk(pb[(int64_t)pid * 3] + off[0], pb[(int64_t)pid * 3 + 1] + off[1],
+                           pb[(int64_t)pid * 3 + 2] + off[2]);
     if (row < 0) continue;
-    // More than 8 slot writes into one dual cube is the reference's "Topology Error"
-    // (dual_mc_inds.cu:86,115,135): the writes are skipped and the count ends above 8,
-    // which the caller can detect from cnt.
-    const int before = atomicAdd(cnt + row, ns);
-    if (before >= 8) continue;
-    for (int i = 0; i < ns; i++) {
-      acc[(row * 8 + slots[i]) * 2] = (int32_t)(pid + idx_base);
-      acc[(row * 8 + slots[i]) * 2 + 1] = depth;
+    atomicAdd(cnt + row, ns);
+    const int2 v = make_int2((int32_t)((int64_t)pid + idx_base), depth);
+    int2* dst = reinterpret_cast<int2*>(acc) + row * 8;
+    dst[slots[0]] = v;
+    if (ns > 1) dst[slots[1]] = v;
+    if (ns > 2) {
+      dst[slots[2]] = v;
+      dst[slots[3]] = v;
     }
   }
+}
+
+// Probes of n_primal cells of stride s: launch over 32-bit indices when they fit.
+template <typename Lookup>
+void launch_dual_inds(Lookup lk, const int32_t* pb, int64_t n_primal, int stride, int depth, int64_t idx_base,
+                      int32_t* acc, int32_t* cnt, cudaStream_t s) {
+  const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
+  const int64_t total = n_primal * per;
+  const unsigned grid = ngs_blocks(total, 256);
+  ngs_count_launch();
+  // 32-bit indexing needs the whole index space plus one grid stride below 2^32
+  if (total + (int64_t)grid * 256 < (int64_t)UINT32_MAX)
+    dual_inds_kernel<Lookup, uint32_t><<<grid, 256, 0, s>>>(lk, pb, (uint32_t)n_primal, stride, depth, idx_base, acc, cnt);
+  else
+    dual_inds_kernel<Lookup, int64_t><<<grid, 256, 0, s>>>(lk, pb, n_primal, stride, depth, idx_base, acc, cnt);
 }
 
 struct GridLookup {
@@ -129,10 +161,9 @@ extern "C" int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_bas
                                         int depth, int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s) {
   if (!dual.words || stride < 1 || n_primal < 0 || (n_primal > 0 && (!primal_base || !acc || !cnt)))
     return NGS_ERR_INVALID_ARG;
+  if (reinterpret_cast<uintptr_t>(acc) & 7u) return NGS_ERR_INVALID_ARG;
   if (n_primal == 0) return NGS_OK;
-  const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
-  { ngs_count_launch(); dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
-      GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, cnt); }
+  launch_dual_inds(GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, cnt, (cudaStream_t)s);
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -142,11 +173,10 @@ extern "C" int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_
                                         ngs_stream s) {
   if (!dual || !dual->slots || stride < 1 || n_primal < 0 || (n_primal > 0 && (!primal_base || !acc || !cnt)))
     return NGS_ERR_INVALID_ARG;
+  if (reinterpret_cast<uintptr_t>(acc) & 7u) return NGS_ERR_INVALID_ARG;
   if (n_primal == 0) return NGS_OK;
-  const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
-  { ngs_count_launch(); dual_inds_kernel<<<ngs_blocks(n_primal * per, 256), 256, 0, (cudaStream_t)s>>>(
-      KeyLookup{static_cast<const Slot*>(dual->slots), dual->nslots - 1}, primal_base, n_primal, stride, depth,
-      idx_base, acc, cnt); }
+  launch_dual_inds(KeyLookup{static_cast<const Slot*>(dual->slots), dual->nslots - 1}, primal_base, n_primal, stride,
+                   depth, idx_base, acc, cnt, (cudaStream_t)s);
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -185,9 +215,15 @@ extern "C" int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, cons
 }
 
 // ----------------------------------------------------------------------------- dual MC
-__global__ void dual_count_kernel(const int32_t* __restrict__ acc, int64_t m, const float* __restrict__ values,
-                                  int32_t* __restrict__ vcount) {
+// cnt (optional): the accumulation counts of an uncompacted acc; cubes whose count is not 8 emit
+// nothing, which leaves the triangles of the others in the order a compacted acc gives them.
+__global__ void dual_count_kernel(const int32_t* __restrict__ acc, const int32_t* __restrict__ cnt, int64_t m,
+                                  const float* __restrict__ values, int32_t* __restrict__ vcount) {
   for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
+    if (cnt && cnt[c] != 8) {
+      vcount[c] = 0;
+      continue;
+    }
     float v[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) v[i] = values[acc[(c * 8 + i) * 2]];
@@ -195,10 +231,12 @@ __global__ void dual_count_kernel(const int32_t* __restrict__ acc, int64_t m, co
   }
 }
 
-__global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int64_t m, const float* __restrict__ pos,
-                                 const float* __restrict__ values, const int64_t* __restrict__ voff,
-                                 float* __restrict__ tris, int32_t* __restrict__ vids) {
+__global__ void dual_emit_kernel(const int32_t* __restrict__ acc, const int32_t* __restrict__ cnt, int64_t m,
+                                 const float* __restrict__ pos, const float* __restrict__ values,
+                                 const int64_t* __restrict__ voff, float* __restrict__ tris,
+                                 int32_t* __restrict__ vids) {
   for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
+    if (cnt && cnt[c] != 8) continue;
     int id[8];
     float v[8];
 #pragma unroll
@@ -225,22 +263,23 @@ __global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int64_t m, con
   }
 }
 
-extern "C" int ngs_dual_mc_count(const int32_t* acc, int64_t n_cubes, const float* values, int32_t* vcount,
-                                 ngs_stream s) {
+extern "C" int ngs_dual_mc_count(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* values,
+                                 int32_t* vcount, ngs_stream s) {
   if (n_cubes < 0 || (n_cubes > 0 && (!acc || !values || !vcount))) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  { ngs_count_launch(); dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, n_cubes, values, vcount); }
+  { ngs_count_launch(); dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, cnt, n_cubes, values, vcount); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
 
-extern "C" int ngs_dual_mc_emit(const int32_t* acc, int64_t n_cubes, const float* pos, const float* values,
-                                const int64_t* voffset, float* tris, int32_t* vert_ids, ngs_stream s) {
+extern "C" int ngs_dual_mc_emit(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* pos,
+                                const float* values, const int64_t* voffset, float* tris, int32_t* vert_ids,
+                                ngs_stream s) {
   if (n_cubes < 0 || (n_cubes > 0 && (!acc || !pos || !values || !voffset || !tris || !vert_ids)))
     return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, n_cubes, pos, values, voffset, tris,
-                                                                        vert_ids); }
+  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, cnt, n_cubes, pos, values,
+                                                                                             voffset, tris, vert_ids); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

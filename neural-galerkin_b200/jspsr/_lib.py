@@ -82,7 +82,7 @@ _SIGS = {
     "ngs_point_basis": ([G, vp, i64, f32, f64, vp, vp, vp], C.c_int),
     "ngs_point_field": ([vp, vp, i64, vp, vp, C.c_int, vp], C.c_int),
     "ngs_eval_field": ([G, vp, i64, f32, f64, vp, C.c_int, vp, vp], C.c_int),
-    "ngs_eval_field_cells": ([C.POINTER(Grid), C.POINTER(vp), C.c_int, i64, C.c_int, vp, f32, f64, vp, vp], C.c_int),
+    "ngs_eval_field_cells": ([C.POINTER(Grid), C.POINTER(vp), C.c_int, i64, vp, f32, f64, vp, vp], C.c_int),
     "ngs_eval_field_levels": ([C.POINTER(Grid), C.POINTER(vp), C.c_int, vp, i64, f32, f64, C.c_int, vp, vp], C.c_int),
     "ngs_weighted_sum": ([vp, vp, i64, vp, vp], C.c_int),
     "ngs_stencil_count": ([G, vp, i64, vp, vp, vp], C.c_int),
@@ -118,8 +118,8 @@ _SIGS = {
     "ngs_dual_mc_indices_hash": ([H, vp, i64, C.c_int, C.c_int, i64, vp, vp, vp], C.c_int),
     "ngs_dual_mc_select": ([vp, i64, vp, vp], C.c_int),
     "ngs_dual_mc_compact": ([vp, vp, vp, i64, vp, vp], C.c_int),
-    "ngs_dual_mc_count": ([vp, i64, vp, vp, vp], C.c_int),
-    "ngs_dual_mc_emit": ([vp, i64, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_count": ([vp, vp, i64, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_emit": ([vp, vp, i64, vp, vp, vp, vp, vp, vp], C.c_int),
     "ngs_vdedup_count": ([vp, i64, vp, vp], C.c_int),
     "ngs_vdedup_sort": ([vp, i64, vp, i64, vp, vp, vp, vp], C.c_int),
     "ngs_vdedup_emit": ([vp, vp, i64, vp, vp, vp, vp, vp, vp, vp], C.c_int),

@@ -447,22 +447,17 @@ class Reconstruction:
                    self.vs, int(grad), L.ptr(out), L.stream())
         return out
 
-    def chi_cells(self, pos: torch.Tensor, starts, counts) -> torch.Tensor:
-        """chi_raw at the 2x2x2 samples of the leaf cells, level by level: segment d of pos (starts[d],
-        counts[d] samples) holds the samples of level-d cells, 8 per cell in expansion order.  The
-        samples of one cell share the neighbourhood of every coarser field level, which is read once
-        per cell."""
+    def chi_cells(self, pos: torch.Tensor) -> torch.Tensor:
+        """chi_raw at the 2x2x2 samples of leaf cells, 8 per cell in expansion order (what
+        ngs_expand_cells writes with n_upsample = 2).  The samples of one cell share the
+        neighbourhood of every field level at least half as fine as the cell, read once per cell."""
         out = torch.zeros(pos.shape[0], dtype=torch.float32, device=self.dev)
-        for d, cnt in enumerate(counts):
-            if cnt == 0:
-                continue
-            seg = slice(int(starts[d]), int(starts[d]) + cnt)
-            for l0 in range(0, len(self.levels), L.MAX_FIELD_LEVELS):
-                lvs = self.levels[l0:l0 + L.MAX_FIELD_LEVELS]
-                grids = (L.Grid * len(lvs))(*[lv.grid for lv in lvs])
-                xs = (L.C.c_void_p * len(lvs))(*[lv.x32.data_ptr() for lv in lvs])
-                L.call("ngs_eval_field_cells", grids, xs, len(lvs), cnt // 8, d - l0, L.ptr(pos[seg]),
-                       np.float32(self.inv_vs), self.vs, L.ptr(out[seg]), L.stream())
+        for l0 in range(0, len(self.levels), L.MAX_FIELD_LEVELS):
+            lvs = self.levels[l0:l0 + L.MAX_FIELD_LEVELS]
+            grids = (L.Grid * len(lvs))(*[lv.grid for lv in lvs])
+            xs = (L.C.c_void_p * len(lvs))(*[lv.x32.data_ptr() for lv in lvs])
+            L.call("ngs_eval_field_cells", grids, xs, len(lvs), pos.shape[0] // 8, L.ptr(pos),
+                   np.float32(self.inv_vs), self.vs, L.ptr(out), L.stream())
         return out
 
     def mean_chi(self) -> torch.Tensor:
@@ -572,25 +567,22 @@ class Reconstruction:
                 L.call("ngs_dual_mc_indices_hash", L.C.byref(table.table), L.ptr(epb[starts[d]:]), counts[d],
                        self.levels[d].stride, d, int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
             self._dual_ws = table
-        keep = torch.empty(nd, dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
-        koff, ktot = L.scan(keep)
-        m = int(ktot.item())
-        acc_c = torch.empty((m, 8, 2), dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_compact", L.ptr(acc), L.ptr(keep), L.ptr(koff), nd, L.ptr(acc_c), st)
+        # the cubes with all 8 corners (cnt == 8) are the reference's compacted list; nearly every
+        # centre is one, so the count and emit passes skip the others in place instead of
+        # compacting acc first (same triangles, same order); dual_cubes() compacts on request
         self.topology_overflow = cnt  # counts above 8 mark the reference's "Topology Error"
         self._mark("dual grid")
         # field at the primal samples
-        vals = (self.chi_cells(pos, starts, counts) if n_upsample == 2 else self.chi_raw(pos)) - mean
+        vals = (self.chi_cells(pos) if n_upsample == 2 else self.chi_raw(pos)) - mean
         self._mark("chi")
         # marching cubes
-        vcount = torch.empty(m, dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_count", L.ptr(acc_c), m, L.ptr(vals), L.ptr(vcount), st)
+        vcount = torch.empty(nd, dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_count", L.ptr(acc), L.ptr(cnt), nd, L.ptr(vals), L.ptr(vcount), st)
         voff, vtot = L.scan(vcount)
         nv = int(vtot.item())
         tris = torch.empty((nv, 3), dtype=torch.float32, device=dev)
         vids = torch.empty((nv, 2), dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_emit", L.ptr(acc_c), m, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris), L.ptr(vids), st)
+        L.call("ngs_dual_mc_emit", L.ptr(acc), L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris), L.ptr(vids), st)
         # vertex de-duplication by (vid0, vid1) (reconstructor.py:380-383)
         bcount = torch.zeros(total, dtype=torch.int32, device=dev)
         L.call("ngs_vdedup_count", L.ptr(vids), nv, L.ptr(bcount), st)
@@ -607,9 +599,23 @@ class Reconstruction:
         L.call("ngs_vdedup_emit", L.ptr(vids), L.ptr(tris), nv, L.ptr(bstart), L.ptr(fill), L.ptr(sorted_keys),
                L.ptr(vid_of), L.ptr(faces), L.ptr(verts), st)
         self._mark("mesh")
-        self.mesh_info = dict(n_primal=total, n_dual=nd, n_cubes=m, max_depth=max_depth, acc=acc_c, values=vals,
+        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_all=acc, cnt=cnt, values=vals,
                               positions=pos, counts=counts)
         return verts, faces.view(-1, 3)
+
+    def dual_cubes(self) -> torch.Tensor:
+        """The complete dual cubes of the last extract_mesh (count 8), in dual-centre order: the
+        reference's compacted [M, 8, 2] (primal id, depth) list (reconstructor.py:366)."""
+        acc, cnt = self.mesh_info["acc_all"], self.mesh_info["cnt"]
+        nd = cnt.shape[0]
+        st = L.stream()
+        keep = torch.empty(nd, dtype=torch.int32, device=self.dev)
+        L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
+        koff, ktot = L.scan(keep)
+        m = int(ktot.item())
+        out = torch.empty((m, 8, 2), dtype=torch.int32, device=self.dev)
+        L.call("ngs_dual_mc_compact", L.ptr(acc), L.ptr(keep), L.ptr(koff), nd, L.ptr(out), st)
+        return out
 
     def _dual_centres_by_sort(self, epb, starts, counts, max_depth, lo, offs):
         """Unique corners of the expanded cells, in lexicographic order, and a key table over them."""

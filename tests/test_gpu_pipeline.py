@@ -103,19 +103,18 @@ def test_dual_grid_bit_exact(cases, gpu_runs, name):
     _, _, mesh = cases[name]
     rec = gpu_runs[name][0]
     assert rec.mesh_info["counts"] == [mesh.n_primal[d] for d in sorted(mesh.n_primal)]
-    np.testing.assert_array_equal(rec.mesh_info["acc"].cpu().numpy(), mesh.acc)
+    np.testing.assert_array_equal(rec.dual_cubes().cpu().numpy(), mesh.acc)
     assert rel(rec.mesh_info["values"].cpu().numpy(), mesh.dual_values) < TOL
 
 
 @pytest.mark.parametrize("name", CASES)
 def test_cell_field_matches_point_field(gpu_runs, name):
-    """The per-cell evaluation of the mesh samples (one neighbourhood read per cell and coarser
-    level) sums the same terms as the per-sample evaluation: equal up to FP32 contraction order."""
+    """The per-cell evaluation of the mesh samples (one neighbourhood read per cell and level,
+    contracted axis by axis) sums the same terms as the per-sample evaluation: equal up to FP32
+    rounding of the different summation order."""
     rec = gpu_runs[name][0]
     info = rec.mesh_info
-    counts = info["counts"]
-    starts = np.concatenate([[0], np.cumsum(counts)])
-    cells = rec.chi_cells(info["positions"], starts, counts).cpu().numpy()
+    cells = rec.chi_cells(info["positions"]).cpu().numpy()
     points = rec.chi_raw(info["positions"]).cpu().numpy()
     assert np.abs(cells - points).max() <= 1e-6 * max(np.abs(points).max(), 1e-30)
 
@@ -185,7 +184,7 @@ def test_sorted_key_dual_centres_match_bitmap(cases, name):
     for max_words in (1 << 27, 0):
         rec.dual_grid_max_words = max_words
         v, f = rec.extract_mesh()
-        out.append((rec.mesh_info["acc"].cpu().numpy(), v.cpu().numpy(), f.cpu().numpy()))
+        out.append((rec.dual_cubes().cpu().numpy(), v.cpu().numpy(), f.cpu().numpy()))
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][2], out[1][2])
     assert np.abs(out[0][1] - out[1][1]).max() <= 1e-5
