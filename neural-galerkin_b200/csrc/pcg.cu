@@ -8,8 +8,9 @@
 //     phase A  (own rows)  p = u + b p;  s = w + b s;  x += a p;  r -= a s;  u = M r
 //     barrier              u visible to every block
 //     phase B  (own rows)  w = A u, partial dots (r,u), (w,u), (r,r)
-//     barrier + reduce     the last block to arrive sums the per-block partials in
-//                          block order (deterministic) and releases the others.
+//     barrier + reduce     every block publishes its partials, arrives, and once all
+//                          have arrived sums all partials itself in block order
+//                          (deterministic, the same bits in every block).
 // The SpMV streams the CSR arrays straight from HBM: eight lanes per row, each lane
 // with up to eight (column, value) pairs and their vector gathers in flight per round, at
 // two blocks per SM.  (Staging CSR tiles through shared memory with bulk copies ran at
@@ -17,8 +18,8 @@
 // the copies, bounded it.)
 // Every wait is bounded by the global nanosecond timer; on timeout the kernel
 // records NGS_ERR_TIMEOUT and returns.  Every solve is bounded too: at most
-// NGS_PCG_ITER_CAP iterations, and a deadline that the last block of each
-// reduction checks, so that all blocks stop at the same iteration.  Dots are
+// NGS_PCG_ITER_CAP iterations, and a deadline that block 0 checks at each
+// reduction and publishes with it, so that all blocks stop at the same iteration.  Dots are
 // FP64 in every mode.
 //
 // Mixed precision (NGS_PCG_MIXED) is iterative refinement: the inner PCG runs on
@@ -60,10 +61,8 @@ struct PcgArgs {
   void* s;
   void* u;
   void* w;
-  double* partials;          // [nblocks][4]
-  double* result;            // [4]
-  unsigned int* count;
-  unsigned int* gen;
+  double* partials;          // [2][nblocks][4]: per-block partial sums, by barrier parity
+  unsigned int* count;       // arrival counter of the grid barriers
   int* error;
   int64_t* info;             // {iters, status, replacements, -}
   double* resid;             // {|r|, |b|}
@@ -72,7 +71,7 @@ struct PcgArgs {
   int replace_every;         // <= 0: never
   double inner_rtol;         // MIXED: relative reduction of an inner solve
   unsigned long long wait_ns;     // bound of one barrier wait
-  unsigned long long* deadline;   // absolute global-timer deadline, set at the first reduction
+  unsigned long long* deadline;   // absolute global-timer deadline, set by block 0 at the first reduction
   unsigned long long budget_ns;   // time budget of the whole solve
   unsigned int nblocks;
   int evict_first;                // stream the matrix past the caches (it does not fit L2)
@@ -164,40 +163,65 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
   __syncthreads();
 }
 
-// Block sums of NV doubles -> per-block partials -> fixed-order grid reduction.
-template <int NV>
-NGS_DEV bool reduce_barrier(const PcgArgs& a, unsigned bid, const double (&v)[NV], double (&out)[NV]) {
-  __shared__ double red[NV > 0 ? NV : 1][PCG_THREADS / 32];
-  __shared__ int last, ok;
-  __shared__ unsigned int gen0;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    const double t = warp_sum(v[k]);
-    if (lane == 0) red[k][wid] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-      double t = 0.0;
-      for (int i = 0; i < PCG_THREADS / 32; i++) t += red[k][i];
-      a.partials[(size_t)bid * 4 + k] = t;
+// Grid synchronisation of a cooperative launch through one arrival counter in global memory (zeroed
+// before the launch, never reset inside it): barrier k of the launch (k = 1, 2, ... -- every block
+// takes the same sequence) is passed once the counter reaches k * nblocks.  Thread 0 of the block
+// arrives and waits; the wait is bounded by the global timer and ends early if another block
+// recorded an error.
+NGS_DEV bool grid_arrive_wait(const PcgArgs& a, unsigned int target) {
+  __threadfence();
+  atomicAdd(a.count, 1u);
+  const unsigned long long t0 = global_ns();
+  while (*reinterpret_cast<volatile unsigned int*>(a.count) < target) {
+    if (*reinterpret_cast<volatile int*>(a.error)) return false;
+    if (global_ns() - t0 > a.wait_ns) {
+      atomicExch(a.error, NGS_ERR_TIMEOUT);
+      return false;
     }
-    gen0 = *reinterpret_cast<volatile unsigned int*>(a.gen);
-    __threadfence();
-    const unsigned int arrived = atomicAdd(a.count, 1u);
-    last = (arrived == a.nblocks - 1);
+    __nanosleep(32);
   }
-  __syncthreads();
-  if (last) {
-    __threadfence();
+  __threadfence();
+  return true;
+}
+
+// Synchronisation of the blocks that solve one system.  GridSync: the blocks of a cooperative
+// launch, through the arrival counter (bounded waits).  A reduction publishes the block's partial
+// sums before arriving, and after the barrier EVERY block sums all blocks' partials itself, in block
+// order with the same code -- the same bits in every block, and no second round trip through a
+// last block that sums and releases the others.  The partials are double-buffered by barrier
+// parity: a block can only write the buffer of reduction k + 2 after every block has arrived at
+// reduction k + 1, that is, after every block has read reduction k.  The solve deadline is decided
+// by block 0 and travels in its partial slot 3, so every block takes the same decision.
+// ClusterSync: the CTAs of one thread-block cluster, through the hardware cluster barrier and
+// distributed shared memory -- no spinning, no co-residency requirement beyond the cluster, which
+// the hardware schedules as a unit.
+struct GridSync {
+  const PcgArgs& a;
+  unsigned bid;
+  unsigned int epoch;
+  bool is_late;
+  NGS_DEV GridSync(const PcgArgs& args, unsigned b) : a(args), bid(b), epoch(0), is_late(false) {}
+
+  NGS_DEV bool barrier() {
+    __shared__ int ok;
+    epoch++;
+    __syncthreads();
+    if (threadIdx.x == 0) ok = grid_arrive_wait(a, epoch * a.nblocks);
+    __syncthreads();
+    return ok != 0;
+  }
+
+  template <int NV>
+  NGS_DEV bool reduce(const double (&v)[NV], double (&out)[NV]) {
+    static_assert(NV <= 3, "slot 3 carries the deadline flag");
+    __shared__ double red[NV][PCG_THREADS / 32];
+    __shared__ int ok;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    epoch++;
+    double* part = a.partials + (size_t)(epoch & 1u) * a.nblocks * 4;
 #pragma unroll
     for (int k = 0; k < NV; k++) {
-      double t = 0.0;
-      for (unsigned int i = threadIdx.x; i < a.nblocks; i += PCG_THREADS) t += ld_cg(a.partials + (size_t)i * 4 + k);
-      t = warp_sum(t);
+      const double t = warp_sum(v[k]);
       if (lane == 0) red[k][wid] = t;
     }
     __syncthreads();
@@ -206,52 +230,37 @@ NGS_DEV bool reduce_barrier(const PcgArgs& a, unsigned bid, const double (&v)[NV
       for (int k = 0; k < NV; k++) {
         double t = 0.0;
         for (int i = 0; i < PCG_THREADS / 32; i++) t += red[k][i];
-        a.result[k] = t;
+        part[(size_t)bid * 4 + k] = t;
       }
-      const unsigned long long now = global_ns();
-      if (*a.deadline == 0ull) *a.deadline = now + a.budget_ns;
-      a.result[3] = now > *a.deadline ? 1.0 : 0.0;   // one decision for every block
-      *a.count = 0;
-      __threadfence();
-      atomicExch(a.gen, gen0 + 1u);
-    }
-  } else if (threadIdx.x == 0) {
-    const unsigned long long t0 = global_ns();
-    while (*reinterpret_cast<volatile unsigned int*>(a.gen) == gen0) {
-      if (*reinterpret_cast<volatile int*>(a.error)) { ok = 0; break; }
-      if (global_ns() - t0 > a.wait_ns) {
-        atomicExch(a.error, NGS_ERR_TIMEOUT);
-        ok = 0;
-        break;
+      if (bid == 0) {
+        const unsigned long long now = global_ns();
+        if (*a.deadline == 0ull) *a.deadline = now + a.budget_ns;
+        part[3] = now > *a.deadline ? 1.0 : 0.0;
       }
-      __nanosleep(32);
+      ok = grid_arrive_wait(a, epoch * a.nblocks);
     }
-    __threadfence();
-  }
-  __syncthreads();
+    __syncthreads();
+    if (!ok) return false;
 #pragma unroll
-  for (int k = 0; k < NV; k++) out[k] = ld_cg(a.result + k);
-  return ok != 0;
-}
-
-NGS_DEV bool plain_barrier(const PcgArgs& a, unsigned bid) {
-  double v[1] = {0.0}, o[1];
-  return reduce_barrier<1>(a, bid, v, o);
-}
-
-NGS_DEV bool past_deadline(const PcgArgs& a) { return ld_cg(a.result + 3) != 0.0; }
-
-// Synchronisation of the blocks that solve one system.  GridSync: the blocks of a cooperative
-// launch, through a counter in global memory (bounded waits).  ClusterSync: the CTAs of one
-// thread-block cluster, through the hardware cluster barrier and distributed shared memory -- no
-// spinning, no co-residency requirement beyond the cluster, which the hardware schedules as a unit.
-struct GridSync {
-  const PcgArgs& a;
-  unsigned bid;
-  template <int NV>
-  NGS_DEV bool reduce(const double (&v)[NV], double (&out)[NV]) { return reduce_barrier<NV>(a, bid, v, out); }
-  NGS_DEV bool barrier() { return plain_barrier(a, bid); }
-  NGS_DEV bool late() const { return past_deadline(a); }
+    for (int k = 0; k < NV; k++) {
+      double t = 0.0;
+      for (unsigned int i = threadIdx.x; i < a.nblocks; i += PCG_THREADS) t += ld_cg(part + (size_t)i * 4 + k);
+      t = warp_sum(t);
+      __syncwarp();
+      if (lane == 0) red[k][wid] = t;
+    }
+    is_late = ld_cg(part + 3) != 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double t = 0.0;
+      for (int i = 0; i < PCG_THREADS / 32; i++) t += red[k][i];
+      out[k] = t;
+    }
+    __syncthreads();            // red is rewritten by the next reduction
+    return true;
+  }
+  NGS_DEV bool late() const { return is_late; }
 };
 
 NGS_DEV void cluster_sync_all() {
@@ -494,7 +503,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
 
 template <int MODE>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_kernel(const __grid_constant__ PcgArgs a) {
-  GridSync sy{a, blockIdx.x};
+  GridSync sy(a, blockIdx.x);
   pcg_body<MODE>(a, blockIdx.x, sy);
 }
 
@@ -525,7 +534,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_batch_kernel(
     const int mid = (lo + hi + 1) >> 1;
     if (b.start[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
   }
-  GridSync sy{b.sys[lo], blockIdx.x - b.start[lo]};
+  GridSync sy(b.sys[lo], blockIdx.x - b.start[lo]);
   pcg_body<MODE>(b.sys[lo], blockIdx.x - b.start[lo], sy);
 }
 
@@ -705,10 +714,8 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.u = base; base += align_up(n * vt);
   a.w = base; base += align_up(n * vt);
   a.partials = reinterpret_cast<double*>(base); base += align_up((size_t)148 * 32 * 4 * sizeof(double));
-  a.result = reinterpret_cast<double*>(base); base += align_up(4 * sizeof(double));
   unsigned int* ctl = reinterpret_cast<unsigned int*>(base);
   a.count = ctl;
-  a.gen = ctl + 1;
   a.error = reinterpret_cast<int*>(ctl + 2);
   a.deadline = reinterpret_cast<unsigned long long*>(ctl + 4);
   a.info = info_dev;
