@@ -44,20 +44,23 @@ __global__ void stencil_count_kernel(ngs_grid g, const int32_t* __restrict__ coo
   for (int64_t i = ngs_gtid() >> 5; i < V; i += warps) {
     int32_t r[5];
     stencil_column(g, coords, i, lane, r);
-    unsigned bal[5];                                  // bal[t] bit l: cell t of lane l's column is present
+    // lane l's column fills mask bits 5l .. 5l+4 (cell t of the column at bit 5l + t); each of the
+    // four 32-bit words is the OR of the lanes' shifted patterns
+    unsigned pat = 0u;
 #pragma unroll
-    for (int t = 0; t < 5; t++) bal[t] = __ballot_sync(0xffffffffu, r[t] >= 0);
+    for (int t = 0; t < 5; t++) pat |= (r[t] >= 0 ? 1u : 0u) << t;
+    const int lo = 5 * lane;
+    unsigned w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int sh = lo - 32 * k;             // position of the pattern's bit 0 in word k
+      const unsigned part = sh >= 32 || sh <= -5 ? 0u : (sh >= 0 ? pat << sh : pat >> -sh);
+      w[k] = __reduce_or_sync(0xffffffffu, part);
+    }
+    const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned)__popc(pat));
     if (lane == 0) {
-      unsigned w[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-      for (int l = 0; l < 25; l++)
-#pragma unroll
-        for (int t = 0; t < 5; t++) {
-          const int o = 5 * l + t;
-          w[o >> 5] |= ((bal[t] >> l) & 1u) << (o & 31);
-        }
       masks[i] = make_uint4(w[0], w[1], w[2], w[3]);
-      counts[i] = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+      counts[i] = (int64_t)total;
     }
   }
 }
@@ -323,12 +326,47 @@ __global__ void rhs_gather_kernel(ngs_grid dg, const float* __restrict__ nrm, co
   }
 }
 
+// target stride == data stride: every data voxel D scatters to the targets D + k stride, k in
+// {-1, 0, 1}^3, so each target T gathers from the data voxels T - k stride instead -- 9 runs of 3
+// cells along z, no atomics, a fixed summation order.  The table index of offset k is k + 1.
+__global__ void rhs_same_level_kernel(ngs_grid dg, const float* __restrict__ nrm, const int32_t* __restrict__ tcoords,
+                                      int64_t nt, const double* __restrict__ tc, const double* __restrict__ tgv,
+                                      double* __restrict__ rhs) {
+  const int s = dg.stride;
+  for (int64_t i = ngs_gtid(); i < nt; i += ngs_gstride()) {
+    const int c0 = tcoords[i * 3], c1 = tcoords[i * 3 + 1], c2 = tcoords[i * 3 + 2];
+    double acc = 0.0;
+#pragma unroll
+    for (int jx = -1; jx <= 1; jx++)
+#pragma unroll
+      for (int jy = -1; jy <= 1; jy++) {
+        int32_t r[3];
+        grid_rows_zrun<3>(dg, c0 + jx * s, c1 + jy * s, c2 - s, r);
+#pragma unroll
+        for (int jz = -1; jz <= 1; jz++) {
+          const int32_t d = r[jz + 1];
+          if (d < 0) continue;
+          // data voxel D = T + j s sees the target at offset k = -j: table index 1 - j
+          const double cx = tc[1 - jx], cy = tc[1 - jy], cz = tc[1 - jz];
+          const double gx = tgv[1 - jx], gy = tgv[1 - jy], gz = tgv[1 - jz];
+          const double n0 = nrm[(int64_t)d * 3], n1 = nrm[(int64_t)d * 3 + 1], n2 = nrm[(int64_t)d * 3 + 2];
+          acc += n0 * gx * cy * cz + n1 * cx * gy * cz + n2 * cx * cy * gz;
+        }
+      }
+    rhs[i] -= acc;
+  }
+}
+
 extern "C" int ngs_rhs_normals(ngs_grid data_grid, const int32_t* data_coords, int64_t n_data, const float* normals,
                                ngs_grid tgt_grid, const int32_t* tgt_coords, int64_t n_tgt, const double* tab_c,
                                const double* tab_g, int tab_len, double* rhs, ngs_stream s) {
   if (!normals || !tab_c || !tab_g || !rhs || tab_len <= 0) return NGS_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)s;
-  if (tgt_grid.stride >= data_grid.stride) {
+  if (tgt_grid.stride == data_grid.stride && tgt_coords && data_grid.words && tab_len == 3) {
+    if (n_tgt <= 0 || n_data <= 0) return NGS_OK;
+    { ngs_count_launch(); rhs_same_level_kernel<<<ngs_blocks(n_tgt, 128), 128, 0, st>>>(data_grid, normals, tgt_coords, n_tgt,
+                                                                                       tab_c, tab_g, rhs); }
+  } else if (tgt_grid.stride >= data_grid.stride) {
     if (n_data <= 0) return NGS_OK;
     if (!data_coords || !tgt_grid.words) return NGS_ERR_INVALID_ARG;
     { ngs_count_launch(); rhs_scatter_kernel<<<ngs_blocks(n_data, 128), 128, 0, st>>>(data_coords, n_data, data_grid.stride, normals,
@@ -372,10 +410,13 @@ __global__ void correction_kernel(const int32_t* __restrict__ fc, int64_t nf, in
       for (int ky = -2; ky <= 2; ky++) {
         const int iy = ky * M + base[1];
         if (iy < 0 || iy >= tab_len) continue;
+        int32_t rz[5];                       // the 5 coarse cells along z, one or two bitmap words
+        grid_rows_zrun<5>(cg, q[0] + kx * sc, q[1] + ky * sc, q[2] - 2 * sc, rz);
+#pragma unroll
         for (int kz = -2; kz <= 2; kz++) {
           const int iz = kz * M + base[2];
           if (iz < 0 || iz >= tab_len) continue;
-          const int64_t j = grid_row(cg, q[0] + kx * sc, q[1] + ky * sc, q[2] + kz * sc);
+          const int64_t j = rz[kz + 2];
           if (j < 0) continue;
           const double v = tabs[tab_len + ix] * tabs[iy] * tabs[iz] + tabs[ix] * tabs[tab_len + iy] * tabs[iz] +
                            tabs[ix] * tabs[iy] * tabs[tab_len + iz];
