@@ -332,23 +332,27 @@ int ngs_primal_mc_count(const float* sdf, int64_t n_cubes, int r, int32_t* vcoun
 int ngs_primal_mc_emit(const float* base, const float* sdf, int64_t n_cubes, int r, const int64_t* voffset,
                        float* tris, int32_t* vert_ids, int32_t* src_ids, float* src_w, ngs_stream s);
 /* Dual-cube corner accumulation for one level of primal cells (expanded units):
- * probes corners / edge / face points of each cell of size `stride` in the
- * dual-centre index and writes (primal id, depth) into acc int32 [D, 8, 2]; cnt int32 [D]. */
+ * probes corners / edge / face points of each cell of size `stride` in the dual-centre index and
+ * writes, per dual cube and slot, slot_words int32: 2 = (primal id, depth) as the reference's
+ * acc int32 [D, 8, 2]; 1 = the primal id alone, acc int32 [D, 8] (all the dual MC passes read).
+ * cnt int32 [D] counts the slot writes; acc must be 8-byte aligned. */
 int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_base, int64_t n_primal, int stride, int depth,
-                             int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s);
+                             int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt, ngs_stream s);
 int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_t* primal_base, int64_t n_primal, int stride,
-                             int depth, int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s);
-/* Keep cubes with cnt == 8: keep_dev int32 flags for a scan, then compaction. */
+                             int depth, int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt, ngs_stream s);
+/* Keep cubes with cnt == 8: keep_dev int32 flags for a scan, then compaction of the rows of
+ * 8 * slot_words int32 (acc and acc_out 16-byte aligned). */
 int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, ngs_stream s);
-int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, const int64_t* keep_offset, int64_t n,
-                        int32_t* acc_out, ngs_stream s);
-/* Dual MC over n_cubes cubes of acc.  cnt (nullable): the accumulation counts of an uncompacted acc;
- * cubes whose count is not 8 emit nothing, so the triangles come out as from the compacted acc and
- * the select / compact pass can be skipped.  NULL: every cube is complete (the reference's op). */
-int ngs_dual_mc_count(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* values, int32_t* vcount,
-                      ngs_stream s);
-int ngs_dual_mc_emit(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* pos, const float* values,
-                     const int64_t* voffset, float* tris, int32_t* vert_ids, ngs_stream s);
+int ngs_dual_mc_compact(const int32_t* acc, int slot_words, const int32_t* keep, const int64_t* keep_offset,
+                        int64_t n, int32_t* acc_out, ngs_stream s);
+/* Dual MC over n_cubes cubes of acc (slot_words as above).  cnt (nullable): the accumulation counts
+ * of an uncompacted acc; cubes whose count is not 8 emit nothing, so the triangles come out as from
+ * the compacted acc and the select / compact pass can be skipped.  NULL: every cube is complete
+ * (the reference's op). */
+int ngs_dual_mc_count(const int32_t* acc, int slot_words, const int32_t* cnt, int64_t n_cubes, const float* values,
+                      int32_t* vcount, ngs_stream s);
+int ngs_dual_mc_emit(const int32_t* acc, int slot_words, const int32_t* cnt, int64_t n_cubes, const float* pos,
+                     const float* values, const int64_t* voffset, float* tris, int32_t* vert_ids, ngs_stream s);
 /* Vertex de-duplication of (vid0, vid1) edge keys (replaces torch.unique(dim=0, return_inverse),
  * ref: jspsr/core/reconstructor.py:380-383): bucket sort by vid0 over n_primal buckets.
  * Phase 1 counts per bucket; the caller scans counts into bucket_start; phase 2 scatters and

@@ -412,15 +412,16 @@ __global__ void correction_kernel(const int32_t* __restrict__ fc, int64_t nf, in
         if (iy < 0 || iy >= tab_len) continue;
         int32_t rz[5];                       // the 5 coarse cells along z, one or two bitmap words
         grid_rows_zrun<5>(cg, q[0] + kx * sc, q[1] + ky * sc, q[2] - 2 * sc, rz);
+        // K = g_x c_y c_z + c_x g_y c_z + c_x c_y g_z = A c_z + B g_z for the column (kx, ky)
+        const double A = tabs[tab_len + ix] * tabs[iy] + tabs[ix] * tabs[tab_len + iy];
+        const double B = tabs[ix] * tabs[iy];
 #pragma unroll
         for (int kz = -2; kz <= 2; kz++) {
           const int iz = kz * M + base[2];
           if (iz < 0 || iz >= tab_len) continue;
           const int64_t j = rz[kz + 2];
           if (j < 0) continue;
-          const double v = tabs[tab_len + ix] * tabs[iy] * tabs[iz] + tabs[ix] * tabs[tab_len + iy] * tabs[iz] +
-                           tabs[ix] * tabs[iy] * tabs[tab_len + iz];
-          acc += v * (double)x[j];
+          acc += (A * tabs[iz] + B * tabs[tab_len + iz]) * (double)x[j];
         }
       }
     }

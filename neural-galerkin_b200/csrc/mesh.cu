@@ -53,7 +53,7 @@ NGS_DEV float sdf_interp(const float* p1, const float* p2, float v1, float v2, f
 // (dual_mc_inds.cu:86,115,135): such a cube's count ends above 8 and the cube is dropped by
 // ngs_dual_mc_select, which keeps the cubes with exactly 8 writes; every probe therefore writes its
 // slots unconditionally and adds to the count without reading it back.
-template <typename Lookup, typename Idx>
+template <typename Lookup, typename Idx, int W>
 __global__ void dual_inds_kernel(Lookup lk, const int32_t* __restrict__ pb, Idx n_primal, int stride, int depth,
                                  int64_t idx_base, int32_t* __restrict__ acc, int32_t* __restrict__ cnt) {
   const Idx sm1 = (Idx)stride - 1;
@@ -115,30 +115,51 @@ __global__ void dual_inds_kernel(Lookup lk, const int32_t* __restrict__ pb, Idx 
                            pb[(int64_t)pid * 3 + 2] + off[2]);
     if (row < 0) continue;
     atomicAdd(cnt + row, ns);
-    const int2 v = make_int2((int32_t)((int64_t)pid + idx_base), depth);
-    int2* dst = reinterpret_cast<int2*>(acc) + row * 8;
-    dst[slots[0]] = v;
-    if (ns > 1) dst[slots[1]] = v;
-    if (ns > 2) {
-      dst[slots[2]] = v;
-      dst[slots[3]] = v;
+    const int32_t id = (int32_t)((int64_t)pid + idx_base);
+    if constexpr (W == 2) {
+      const int2 v = make_int2(id, depth);
+      int2* dst = reinterpret_cast<int2*>(acc) + row * 8;
+      dst[slots[0]] = v;
+      if (ns > 1) dst[slots[1]] = v;
+      if (ns > 2) {
+        dst[slots[2]] = v;
+        dst[slots[3]] = v;
+      }
+    } else {
+      int32_t* dst = acc + row * 8;
+      dst[slots[0]] = id;
+      if (ns > 1) dst[slots[1]] = id;
+      if (ns > 2) {
+        dst[slots[2]] = id;
+        dst[slots[3]] = id;
+      }
     }
   }
 }
 
 // Probes of n_primal cells of stride s: launch over 32-bit indices when they fit.
-template <typename Lookup>
-void launch_dual_inds(Lookup lk, const int32_t* pb, int64_t n_primal, int stride, int depth, int64_t idx_base,
-                      int32_t* acc, int32_t* cnt, cudaStream_t s) {
+template <typename Lookup, int W>
+void launch_dual_inds_w(Lookup lk, const int32_t* pb, int64_t n_primal, int stride, int depth, int64_t idx_base,
+                        int32_t* acc, int32_t* cnt, cudaStream_t s) {
   const int64_t per = 8 + 12 * (int64_t)(stride - 1) + 6 * (int64_t)(stride - 1) * (stride - 1);
   const int64_t total = n_primal * per;
   const unsigned grid = ngs_blocks(total, 256);
   ngs_count_launch();
   // 32-bit indexing needs the whole index space plus one grid stride below 2^32
   if (total + (int64_t)grid * 256 < (int64_t)UINT32_MAX)
-    dual_inds_kernel<Lookup, uint32_t><<<grid, 256, 0, s>>>(lk, pb, (uint32_t)n_primal, stride, depth, idx_base, acc, cnt);
+    dual_inds_kernel<Lookup, uint32_t, W><<<grid, 256, 0, s>>>(lk, pb, (uint32_t)n_primal, stride, depth, idx_base, acc,
+                                                               cnt);
   else
-    dual_inds_kernel<Lookup, int64_t><<<grid, 256, 0, s>>>(lk, pb, n_primal, stride, depth, idx_base, acc, cnt);
+    dual_inds_kernel<Lookup, int64_t, W><<<grid, 256, 0, s>>>(lk, pb, n_primal, stride, depth, idx_base, acc, cnt);
+}
+
+// slot_words 2: the reference's (primal id, depth) pairs; 1: primal ids alone (the dual MC passes
+// read nothing else)
+template <typename Lookup>
+void launch_dual_inds(Lookup lk, const int32_t* pb, int64_t n_primal, int stride, int depth, int64_t idx_base,
+                      int32_t* acc, int slot_words, int32_t* cnt, cudaStream_t s) {
+  if (slot_words == 2) launch_dual_inds_w<Lookup, 2>(lk, pb, n_primal, stride, depth, idx_base, acc, cnt, s);
+  else launch_dual_inds_w<Lookup, 1>(lk, pb, n_primal, stride, depth, idx_base, acc, cnt, s);
 }
 
 struct GridLookup {
@@ -158,25 +179,27 @@ struct KeyLookup {
 };
 
 extern "C" int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_base, int64_t n_primal, int stride,
-                                        int depth, int64_t idx_base, int32_t* acc, int32_t* cnt, ngs_stream s) {
+                                        int depth, int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt,
+                                        ngs_stream s) {
   if (!dual.words || stride < 1 || n_primal < 0 || (n_primal > 0 && (!primal_base || !acc || !cnt)))
     return NGS_ERR_INVALID_ARG;
-  if (reinterpret_cast<uintptr_t>(acc) & 7u) return NGS_ERR_INVALID_ARG;
+  if ((slot_words != 1 && slot_words != 2) || (reinterpret_cast<uintptr_t>(acc) & 7u)) return NGS_ERR_INVALID_ARG;
   if (n_primal == 0) return NGS_OK;
-  launch_dual_inds(GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, cnt, (cudaStream_t)s);
+  launch_dual_inds(GridLookup{dual}, primal_base, n_primal, stride, depth, idx_base, acc, slot_words, cnt,
+                   (cudaStream_t)s);
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
 
 extern "C" int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_t* primal_base, int64_t n_primal,
-                                        int stride, int depth, int64_t idx_base, int32_t* acc, int32_t* cnt,
-                                        ngs_stream s) {
+                                        int stride, int depth, int64_t idx_base, int32_t* acc, int slot_words,
+                                        int32_t* cnt, ngs_stream s) {
   if (!dual || !dual->slots || stride < 1 || n_primal < 0 || (n_primal > 0 && (!primal_base || !acc || !cnt)))
     return NGS_ERR_INVALID_ARG;
-  if (reinterpret_cast<uintptr_t>(acc) & 7u) return NGS_ERR_INVALID_ARG;
+  if ((slot_words != 1 && slot_words != 2) || (reinterpret_cast<uintptr_t>(acc) & 7u)) return NGS_ERR_INVALID_ARG;
   if (n_primal == 0) return NGS_OK;
   launch_dual_inds(KeyLookup{static_cast<const Slot*>(dual->slots), dual->nslots - 1}, primal_base, n_primal, stride,
-                   depth, idx_base, acc, cnt, (cudaStream_t)s);
+                   depth, idx_base, acc, slot_words, cnt, (cudaStream_t)s);
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -185,14 +208,14 @@ __global__ void select_kernel(const int32_t* __restrict__ cnt, int64_t n, int32_
   for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) keep[i] = cnt[i] == 8 ? 1 : 0;
 }
 
-__global__ void compact_acc_kernel(const int32_t* __restrict__ acc, const int32_t* __restrict__ keep,
+// rows of 8 * slot_words int32 (32 or 64 bytes), copied as int4
+__global__ void compact_acc_kernel(const int32_t* __restrict__ acc, int quads, const int32_t* __restrict__ keep,
                                    const int64_t* __restrict__ off, int64_t n, int32_t* __restrict__ out) {
   for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
     if (!keep[i]) continue;
-    const int4* src = reinterpret_cast<const int4*>(acc + i * 16);
-    int4* dst = reinterpret_cast<int4*>(out + off[i] * 16);
-#pragma unroll
-    for (int k = 0; k < 4; k++) dst[k] = src[k];
+    const int4* src = reinterpret_cast<const int4*>(acc) + i * quads;
+    int4* dst = reinterpret_cast<int4*>(out) + off[i] * quads;
+    for (int k = 0; k < quads; k++) dst[k] = src[k];
   }
 }
 
@@ -204,12 +227,14 @@ extern "C" int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, 
   return NGS_OK;
 }
 
-extern "C" int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, const int64_t* keep_offset, int64_t n,
-                                   int32_t* acc_out, ngs_stream s) {
+extern "C" int ngs_dual_mc_compact(const int32_t* acc, int slot_words, const int32_t* keep, const int64_t* keep_offset,
+                                   int64_t n, int32_t* acc_out, ngs_stream s) {
   if (n < 0 || (n > 0 && (!acc || !keep || !keep_offset || !acc_out))) return NGS_ERR_INVALID_ARG;
+  if (slot_words != 1 && slot_words != 2) return NGS_ERR_INVALID_ARG;
   if ((reinterpret_cast<uintptr_t>(acc) | reinterpret_cast<uintptr_t>(acc_out)) & 15u) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  { ngs_count_launch(); compact_acc_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(acc, keep, keep_offset, n, acc_out); }
+  { ngs_count_launch(); compact_acc_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(acc, 2 * slot_words, keep, keep_offset, n,
+                                                                                     acc_out); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -217,7 +242,7 @@ extern "C" int ngs_dual_mc_compact(const int32_t* acc, const int32_t* keep, cons
 // ----------------------------------------------------------------------------- dual MC
 // cnt (optional): the accumulation counts of an uncompacted acc; cubes whose count is not 8 emit
 // nothing, which leaves the triangles of the others in the order a compacted acc gives them.
-__global__ void dual_count_kernel(const int32_t* __restrict__ acc, const int32_t* __restrict__ cnt, int64_t m,
+__global__ void dual_count_kernel(const int32_t* __restrict__ acc, int W, const int32_t* __restrict__ cnt, int64_t m,
                                   const float* __restrict__ values, int32_t* __restrict__ vcount) {
   for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
     if (cnt && cnt[c] != 8) {
@@ -226,12 +251,12 @@ __global__ void dual_count_kernel(const int32_t* __restrict__ acc, const int32_t
     }
     float v[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = values[acc[(c * 8 + i) * 2]];
+    for (int i = 0; i < 8; i++) v[i] = values[acc[(c * 8 + i) * W]];
     vcount[c] = num_verts(cube_type(v));
   }
 }
 
-__global__ void dual_emit_kernel(const int32_t* __restrict__ acc, const int32_t* __restrict__ cnt, int64_t m,
+__global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int W, const int32_t* __restrict__ cnt, int64_t m,
                                  const float* __restrict__ pos, const float* __restrict__ values,
                                  const int64_t* __restrict__ voff, float* __restrict__ tris,
                                  int32_t* __restrict__ vids) {
@@ -241,7 +266,7 @@ __global__ void dual_emit_kernel(const int32_t* __restrict__ acc, const int32_t*
     float v[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-      id[i] = acc[(c * 8 + i) * 2];
+      id[i] = acc[(c * 8 + i) * W];
       v[i] = values[id[i]];
     }
     const int t = cube_type(v);
@@ -263,22 +288,25 @@ __global__ void dual_emit_kernel(const int32_t* __restrict__ acc, const int32_t*
   }
 }
 
-extern "C" int ngs_dual_mc_count(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* values,
-                                 int32_t* vcount, ngs_stream s) {
+extern "C" int ngs_dual_mc_count(const int32_t* acc, int slot_words, const int32_t* cnt, int64_t n_cubes,
+                                 const float* values, int32_t* vcount, ngs_stream s) {
   if (n_cubes < 0 || (n_cubes > 0 && (!acc || !values || !vcount))) return NGS_ERR_INVALID_ARG;
+  if (slot_words != 1 && slot_words != 2) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  { ngs_count_launch(); dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, cnt, n_cubes, values, vcount); }
+  { ngs_count_launch(); dual_count_kernel<<<ngs_blocks(n_cubes, 256), 256, 0, (cudaStream_t)s>>>(acc, slot_words, cnt, n_cubes, values,
+                                                                                    vcount); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
 
-extern "C" int ngs_dual_mc_emit(const int32_t* acc, const int32_t* cnt, int64_t n_cubes, const float* pos,
-                                const float* values, const int64_t* voffset, float* tris, int32_t* vert_ids,
-                                ngs_stream s) {
+extern "C" int ngs_dual_mc_emit(const int32_t* acc, int slot_words, const int32_t* cnt, int64_t n_cubes,
+                                const float* pos, const float* values, const int64_t* voffset, float* tris,
+                                int32_t* vert_ids, ngs_stream s) {
   if (n_cubes < 0 || (n_cubes > 0 && (!acc || !pos || !values || !voffset || !tris || !vert_ids)))
     return NGS_ERR_INVALID_ARG;
+  if (slot_words != 1 && slot_words != 2) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, cnt, n_cubes, pos, values,
+  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, slot_words, cnt, n_cubes, pos, values,
                                                                                              voffset, tris, vert_ids); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;

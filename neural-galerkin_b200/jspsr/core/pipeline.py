@@ -549,11 +549,11 @@ class Reconstruction:
             dcount = torch.empty(1, dtype=torch.int64, device=dev)
             self._dual_ws = L.grid_finalize(dg, dw, dcount)
             nd = int(dcount.item())
-            acc = torch.zeros((nd, 8, 2), dtype=torch.int32, device=dev)
+            acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
             cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
             for d in range(max_depth):
                 L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride, d,
-                       int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
+                       int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
         else:
             # deep hierarchies: the coarse cells stretch the box far beyond the surface, so the
             # dual centres are de-duplicated by a sort of packed corner keys and found through the
@@ -561,11 +561,11 @@ class Reconstruction:
             if np.any(dims >= (1 << 21)):
                 raise ValueError(f"mesh domain of {dims.tolist()} cells exceeds 2^21 cells per axis")
             nd, table = self._dual_centres_by_sort(epb, starts, counts, max_depth, lo, offs)
-            acc = torch.zeros((nd, 8, 2), dtype=torch.int32, device=dev)
+            acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
             cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
             for d in range(max_depth):
                 L.call("ngs_dual_mc_indices_hash", L.C.byref(table.table), L.ptr(epb[starts[d]:]), counts[d],
-                       self.levels[d].stride, d, int(starts[d]), L.ptr(acc), L.ptr(cnt), st)
+                       self.levels[d].stride, d, int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
             self._dual_ws = table
         # the cubes with all 8 corners (cnt == 8) are the reference's compacted list; nearly every
         # centre is one, so the count and emit passes skip the others in place instead of
@@ -577,12 +577,12 @@ class Reconstruction:
         self._mark("chi")
         # marching cubes
         vcount = torch.empty(nd, dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_count", L.ptr(acc), L.ptr(cnt), nd, L.ptr(vals), L.ptr(vcount), st)
+        L.call("ngs_dual_mc_count", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(vals), L.ptr(vcount), st)
         voff, vtot = L.scan(vcount)
         nv = int(vtot.item())
         tris = torch.empty((nv, 3), dtype=torch.float32, device=dev)
         vids = torch.empty((nv, 2), dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_emit", L.ptr(acc), L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris), L.ptr(vids), st)
+        L.call("ngs_dual_mc_emit", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris), L.ptr(vids), st)
         # vertex de-duplication by (vid0, vid1) (reconstructor.py:380-383)
         bcount = torch.zeros(total, dtype=torch.int32, device=dev)
         L.call("ngs_vdedup_count", L.ptr(vids), nv, L.ptr(bcount), st)
@@ -599,23 +599,26 @@ class Reconstruction:
         L.call("ngs_vdedup_emit", L.ptr(vids), L.ptr(tris), nv, L.ptr(bstart), L.ptr(fill), L.ptr(sorted_keys),
                L.ptr(vid_of), L.ptr(faces), L.ptr(verts), st)
         self._mark("mesh")
-        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_all=acc, cnt=cnt, values=vals,
-                              positions=pos, counts=counts)
+        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_ids=acc, cnt=cnt, values=vals,
+                              positions=pos, counts=counts, starts=starts)
         return verts, faces.view(-1, 3)
 
     def dual_cubes(self) -> torch.Tensor:
         """The complete dual cubes of the last extract_mesh (count 8), in dual-centre order: the
         reference's compacted [M, 8, 2] (primal id, depth) list (reconstructor.py:366)."""
-        acc, cnt = self.mesh_info["acc_all"], self.mesh_info["cnt"]
+        acc, cnt = self.mesh_info["acc_ids"], self.mesh_info["cnt"]
         nd = cnt.shape[0]
         st = L.stream()
         keep = torch.empty(nd, dtype=torch.int32, device=self.dev)
         L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
         koff, ktot = L.scan(keep)
         m = int(ktot.item())
-        out = torch.empty((m, 8, 2), dtype=torch.int32, device=self.dev)
-        L.call("ngs_dual_mc_compact", L.ptr(acc), L.ptr(keep), L.ptr(koff), nd, L.ptr(out), st)
-        return out
+        ids = torch.empty((m, 8), dtype=torch.int32, device=self.dev)
+        L.call("ngs_dual_mc_compact", L.ptr(acc), 1, L.ptr(keep), L.ptr(koff), nd, L.ptr(ids), st)
+        # the depth of a primal sample is the level whose segment holds its id
+        bounds = torch.as_tensor(np.asarray(self.mesh_info["starts"][1:], dtype=np.int64), device=self.dev)
+        depth = torch.bucketize(ids.long(), bounds, right=True).int()
+        return torch.stack([ids, depth], dim=2)
 
     def _dual_centres_by_sort(self, epb, starts, counts, max_depth, lo, offs):
         """Unique corners of the expanded cells, in lexicographic order, and a key table over them."""

@@ -249,12 +249,12 @@ def dual_marching_cubes_sparse(cube_corner_inds: torch.Tensor, corner_pos: torch
     M = acc.shape[0]
     dev = acc.device
     vc = torch.empty(M, dtype=torch.int32, device=dev)
-    L.call("ngs_dual_mc_count", L.ptr(acc), None, M, L.ptr(val), L.ptr(vc), L.stream())
+    L.call("ngs_dual_mc_count", L.ptr(acc), 2, None, M, L.ptr(val), L.ptr(vc), L.stream())
     off, tot = L.scan(vc)
     nv = int(tot.item())
     tris = torch.empty((nv // 3, 3, 3), dtype=torch.float32, device=dev)
     vids = torch.empty((nv // 3, 3, 2), dtype=torch.int32, device=dev)
-    L.call("ngs_dual_mc_emit", L.ptr(acc), None, M, L.ptr(pos), L.ptr(val), L.ptr(off), L.ptr(tris), L.ptr(vids), L.stream())
+    L.call("ngs_dual_mc_emit", L.ptr(acc), 2, None, M, L.ptr(pos), L.ptr(val), L.ptr(off), L.ptr(tris), L.ptr(vids), L.stream())
     return [tris, vids]
 
 
@@ -268,7 +268,7 @@ def dual_marching_cubes_indices(dual_centers_hash_data: HashLookupData, expand_p
     for d, stride in primal_strides.items():
         base = expand_primal_base[d].contiguous().int()
         L.call("ngs_dual_mc_indices_hash", C.byref(dual_centers_hash_data.table), L.ptr(base), base.shape[0],
-               int(stride), int(d), int(primal_inds_base[d]), L.ptr(acc), L.ptr(cnt), L.stream())
+               int(stride), int(d), int(primal_inds_base[d]), L.ptr(acc), 2, L.ptr(cnt), L.stream())
     return [acc, cnt]
 
 
