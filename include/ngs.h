@@ -114,6 +114,9 @@ int ngs_grid_mark_points(ngs_grid g, const float* xyz, int64_t n, float inv_vs, 
 /* Mark coords[i] + offsets[j] * offset_scale for every i, j (offsets int32 [n_off, 3]; NULL = origin). */
 int ngs_grid_mark_coords(ngs_grid g, const int32_t* coords, int64_t n, const int32_t* offsets, int n_off,
                          int offset_scale, ngs_stream s);
+/* Mark cells[i] * 2 + {0, stride, 2 stride}^3: the corners of the 2x2x2 expanded samples of each cell
+ * (the same cells as ngs_grid_mark_coords on the expanded samples with the 8 unit offsets). */
+int ngs_grid_mark_cell_corners(ngs_grid g, const int32_t* cells, int64_t n, int stride, ngs_stream s);
 size_t ngs_grid_workspace_bytes(const ngs_grid* g);
 /* Prefix counts over the words; *count_dev (int64) receives the number of cells set. */
 int ngs_grid_finalize(ngs_grid g, void* ws, size_t ws_bytes, int64_t* count_dev, ngs_stream s);
@@ -340,6 +343,11 @@ int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_base, int64_t 
                              int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt, ngs_stream s);
 int ngs_dual_mc_indices_hash(const ngs_hash_table* dual, const int32_t* primal_base, int64_t n_primal, int stride,
                              int depth, int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt, ngs_stream s);
+/* The same accumulation for level-0 leaf cells (cell stride 1, n_up = 2) given as cells, not as
+ * expanded samples: the 8 samples of cell i have ids idx_base + 8 i + e (ngs_expand_cells order);
+ * each of a cell's 27 sample corners is looked up once.  dual must have stride 1. */
+int ngs_dual_mc_indices_cells(ngs_grid dual, const int32_t* cells, int64_t n_cells, int depth, int64_t idx_base,
+                              int32_t* acc, int slot_words, int32_t* cnt, ngs_stream s);
 /* Keep cubes with cnt == 8: keep_dev int32 flags for a scan, then compaction of the rows of
  * 8 * slot_words int32 (acc and acc_out 16-byte aligned). */
 int ngs_dual_mc_select(const int32_t* cnt, int64_t n, int32_t* keep, ngs_stream s);

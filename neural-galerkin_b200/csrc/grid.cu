@@ -45,6 +45,38 @@ __global__ void mark_coords_kernel(ngs_grid g, const int32_t* __restrict__ c, in
   }
 }
 
+// The 27 lattice points c * 2 + {0, s, 2s}^3 of each cell: the corners of the cell's 2 x 2 x 2
+// expanded samples (n_up = 2), what marking every sample's 8 corners sets.  One thread per (cell,
+// x, y) column: the column's three z points usually share a bitmap word and take one atomic.
+__global__ void mark_cell_corners_kernel(ngs_grid g, const int32_t* __restrict__ c, int64_t n, int s) {
+  const int64_t total = n * 9;
+  for (int64_t t = ngs_gtid(); t < total; t += ngs_gstride()) {
+    const int64_t i = t / 9;
+    const int col = (int)(t - i * 9);
+    const int x = c[i * 3] * 2 + (col / 3) * s, y = c[i * 3 + 1] * 2 + (col % 3) * s, z0 = c[i * 3 + 2] * 2;
+    int64_t have = -1;
+    unsigned long long m = 0ull;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      int bit;
+      const int64_t w = grid_word_index(g, x, y, z0 + k * s, &bit);
+      if (w != have) {
+        if (have >= 0) {
+          unsigned long long* bits = reinterpret_cast<unsigned long long*>(static_cast<char*>(g.words) + have * 16 + 8);
+          if ((*reinterpret_cast<volatile unsigned long long*>(bits) & m) != m) atomicOr(bits, m);
+        }
+        have = w;
+        m = 0ull;
+      }
+      if (w >= 0) m |= 1ull << bit;
+    }
+    if (have >= 0) {
+      unsigned long long* bits = reinterpret_cast<unsigned long long*>(static_cast<char*>(g.words) + have * 16 + 8);
+      if ((*reinterpret_cast<volatile unsigned long long*>(bits) & m) != m) atomicOr(bits, m);
+    }
+  }
+}
+
 struct WordPopc {
   const GridWord* w;
   NGS_DEV int64_t operator()(int64_t i) const { return __popcll(w[i].bits); }
@@ -104,6 +136,14 @@ extern "C" int ngs_grid_mark_coords(ngs_grid g, const int32_t* coords, int64_t n
   if (n == 0 || n_off <= 0) return NGS_OK;
   { ngs_count_launch(); mark_coords_kernel<<<ngs_blocks(n * n_off, 256), 256, 0, (cudaStream_t)s>>>(g, coords, n, offsets, n_off,
                                                                              offset_scale); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+extern "C" int ngs_grid_mark_cell_corners(ngs_grid g, const int32_t* cells, int64_t n, int stride, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || stride < 1 || (n > 0 && !cells)) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  { ngs_count_launch(); mark_cell_corners_kernel<<<ngs_blocks(n * 9, 256), 256, 0, (cudaStream_t)s>>>(g, cells, n, stride); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -212,9 +252,11 @@ struct PointNbr {
 NGS_DEV void axis_nbr(float p, float inv_vs, double vs, int stride, float inv_s, int& q, float (&rel)[3]) {
   q = point_quant(q32(p, inv_vs), stride, inv_s);
   const double pos = (double)p / vs - 0.5;
+  // strides are powers of two: scaling by the reciprocal is exact, the same bits as the division
+  const double is = 1.0 / (double)stride;
 #pragma unroll
   for (int k = 0; k < 3; k++)
-    rel[k] = (float)((pos - (double)q - (double)((k - 1) * stride) - 0.5 * (stride - 1)) / stride);
+    rel[k] = (float)((pos - (double)q - (double)((k - 1) * stride) - 0.5 * (stride - 1)) * is);
 }
 
 NGS_DEV PointNbr point_nbr(const float* p, float inv_vs, double vs, int stride) {

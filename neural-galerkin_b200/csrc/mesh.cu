@@ -178,6 +178,60 @@ struct KeyLookup {
   }
 };
 
+// Level-0 cells (stride 1: every probe is a sample corner) taken a cell at a time: the 8 expanded
+// samples of cell i (ids idx_base + 8 i + e, e = ex*4 + ey*2 + ez) have their corners on the
+// lattice c * 2 + p, p in {0,1,2}^3.  Each of the 27 lattice points is looked up once (9 runs of 3
+// along z) and takes one count update for all the samples that touch it; sample e reaches point p
+// through its corner q = p - e, which fills the slot of the octant opposite q -- the same slots and
+// counts as the per-sample probes of dual_inds_kernel.
+template <int W>
+__global__ void dual_inds_cells_kernel(ngs_grid dual, const int32_t* __restrict__ cells, int64_t n, int depth,
+                                       int64_t idx_base, int32_t* __restrict__ acc, int32_t* __restrict__ cnt) {
+  for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
+    const int x0 = cells[i * 3] * 2, y0 = cells[i * 3 + 1] * 2, z0 = cells[i * 3 + 2] * 2;
+    const int64_t id0 = idx_base + i * 8;
+#pragma unroll 1
+    for (int pxy = 0; pxy < 9; pxy++) {
+      const int px = pxy / 3, py = pxy % 3;
+      int32_t r[3];
+      grid_rows_zrun<3>(dual, x0 + px, y0 + py, z0, r);
+#pragma unroll
+      for (int pz = 0; pz < 3; pz++) {
+        const int64_t row = r[pz];
+        if (row < 0) continue;
+        const int nx = px == 1 ? 2 : 1, ny = py == 1 ? 2 : 1, nz = pz == 1 ? 2 : 1;
+        atomicAdd(cnt + row, nx * ny * nz);
+        for (int ex = px == 2 ? 1 : 0; ex <= (px == 0 ? 0 : 1); ex++)
+          for (int ey = py == 2 ? 1 : 0; ey <= (py == 0 ? 0 : 1); ey++)
+            for (int ez = pz == 2 ? 1 : 0; ez <= (pz == 0 ? 0 : 1); ez++) {
+              const int qx = px - ex, qy = py - ey, qz = pz - ez;
+              const int slot = c_octant_slot[(1 - qx) + 2 * (1 - qy) + 4 * (1 - qz)];
+              const int32_t id = (int32_t)(id0 + ex * 4 + ey * 2 + ez);
+              if constexpr (W == 2) reinterpret_cast<int2*>(acc)[row * 8 + slot] = make_int2(id, depth);
+              else acc[row * 8 + slot] = id;
+            }
+      }
+    }
+  }
+}
+
+extern "C" int ngs_dual_mc_indices_cells(ngs_grid dual, const int32_t* cells, int64_t n_cells, int depth,
+                                         int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt, ngs_stream s) {
+  if (!dual.words || dual.stride != 1 || n_cells < 0 || (n_cells > 0 && (!cells || !acc || !cnt)))
+    return NGS_ERR_INVALID_ARG;
+  if ((slot_words != 1 && slot_words != 2) || (reinterpret_cast<uintptr_t>(acc) & 7u)) return NGS_ERR_INVALID_ARG;
+  if (n_cells == 0) return NGS_OK;
+  ngs_count_launch();
+  if (slot_words == 2)
+    dual_inds_cells_kernel<2><<<ngs_blocks(n_cells, 128), 128, 0, (cudaStream_t)s>>>(dual, cells, n_cells, depth,
+                                                                                     idx_base, acc, cnt);
+  else
+    dual_inds_cells_kernel<1><<<ngs_blocks(n_cells, 128), 128, 0, (cudaStream_t)s>>>(dual, cells, n_cells, depth,
+                                                                                     idx_base, acc, cnt);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
 extern "C" int ngs_dual_mc_indices_grid(ngs_grid dual, const int32_t* primal_base, int64_t n_primal, int stride,
                                         int depth, int64_t idx_base, int32_t* acc, int slot_words, int32_t* cnt,
                                         ngs_stream s) {

@@ -114,6 +114,8 @@ _SIGS = {
     "ngs_ddi_backward": ([vp, vp, vp, vp, vp, vp, vp, i64, C.c_int, C.c_int, vp, vp, vp], C.c_int),
     "ngs_primal_mc_count": ([vp, i64, C.c_int, vp, vp], C.c_int),
     "ngs_primal_mc_emit": ([vp, vp, i64, C.c_int, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_dual_mc_indices_cells": ([G, vp, i64, C.c_int, i64, vp, C.c_int, vp, vp], C.c_int),
+    "ngs_grid_mark_cell_corners": ([G, vp, i64, C.c_int, vp], C.c_int),
     "ngs_dual_mc_indices_grid": ([G, vp, i64, C.c_int, C.c_int, i64, vp, C.c_int, vp, vp], C.c_int),
     "ngs_dual_mc_indices_hash": ([H, vp, i64, C.c_int, C.c_int, i64, vp, C.c_int, vp, vp], C.c_int),
     "ngs_dual_mc_select": ([vp, i64, vp, vp], C.c_int),

@@ -544,16 +544,23 @@ class Reconstruction:
             # rank bitmap over the box: dual centres ranked without a sort
             dg, dw = L.make_grid(lo, dims, 1, dev)
             for d in range(max_depth):
-                L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
-                       self.levels[d].stride, st)
+                if n_upsample == 2:
+                    L.call("ngs_grid_mark_cell_corners", dg, L.ptr(base[d]), base[d].shape[0], self.levels[d].stride, st)
+                else:
+                    L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
+                           self.levels[d].stride, st)
             dcount = torch.empty(1, dtype=torch.int64, device=dev)
             self._dual_ws = L.grid_finalize(dg, dw, dcount)
             nd = int(dcount.item())
             acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
             cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
             for d in range(max_depth):
-                L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride, d,
-                       int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
+                if n_upsample == 2 and self.levels[d].stride == 1:
+                    L.call("ngs_dual_mc_indices_cells", dg, L.ptr(base[d]), base[d].shape[0], d, int(starts[d]),
+                           L.ptr(acc), 1, L.ptr(cnt), st)
+                else:
+                    L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride,
+                           d, int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
         else:
             # deep hierarchies: the coarse cells stretch the box far beyond the surface, so the
             # dual centres are de-duplicated by a sort of packed corner keys and found through the
@@ -582,7 +589,8 @@ class Reconstruction:
         nv = int(vtot.item())
         tris = torch.empty((nv, 3), dtype=torch.float32, device=dev)
         vids = torch.empty((nv, 2), dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_emit", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris), L.ptr(vids), st)
+        L.call("ngs_dual_mc_emit", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris),
+               L.ptr(vids), st)
         # vertex de-duplication by (vid0, vid1) (reconstructor.py:380-383)
         bcount = torch.zeros(total, dtype=torch.int32, device=dev)
         L.call("ngs_vdedup_count", L.ptr(vids), nv, L.ptr(bcount), st)
