@@ -23,8 +23,9 @@
 // FP64 in every mode.
 //
 // Mixed precision (NGS_PCG_MIXED) is iterative refinement: the inner PCG runs on
-// the FP32 matrix with FP32 search vectors, FP64 accumulation of every product
-// and dot, and FP64 x and r, until its residual has dropped by `inner_rtol`; then
+// the FP32 matrix with FP32 search vectors (SpMV products summed in FP32 over rounds
+// of eight, the rounds in FP64), FP64 dots, and FP64 x and r, until its residual
+// has dropped by `inner_rtol`; then
 // the true residual b - A x is formed with the FP64 matrix and the inner solve
 // restarts from it.  The FP32 matrix is a fixed SPD perturbation of the FP64 one,
 // so each outer step contracts the error by about |A32 - A64| |A64^-1| and the
@@ -122,6 +123,7 @@ NGS_DEV bool block_rows(const PcgArgs& a, unsigned bid, int64_t& row0, int64_t& 
 template <typename T>
 NGS_DEV T ld_mat(const T* p, bool stream) { return stream ? __ldcs(p) : __ldg(p); }
 
+
 // y = A v over rows [row0, row1): eight lanes per row.  epi(row, acc, pre(row)) consumes each
 // row's product (lane 0 of its group) and returns a contribution to the thread's partial sum.
 // The gathered vector is read with plain loads: it was written earlier in this launch.  Ends with a
@@ -152,8 +154,16 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
       VT xv[U];
 #pragma unroll
       for (int k = 0; k < U; k++) xv[k] = c[k] >= 0 ? v[c[k]] : (VT)0;
+      // the round's products summed in the matrix type (two chains), the round sum accumulated in ACC:
+      // one conversion per round instead of two per product; the FP64 refinement of the mixed mode
+      // works from the true residual, so this rounding only shapes the inner iterations
+      MT r0 = (MT)0, r1 = (MT)0;
 #pragma unroll
-      for (int k = 0; k < U; k++) acc += (ACC)m[k] * (ACC)xv[k];
+      for (int k = 0; k < U; k += 2) {
+        r0 += m[k] * (MT)xv[k];
+        r1 += m[k + 1] * (MT)xv[k + 1];
+      }
+      acc += (ACC)r0 + (ACC)r1;
     }
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
