@@ -120,17 +120,19 @@ NGS_DEV bool block_rows(const PcgArgs& a, unsigned bid, int64_t& row0, int64_t& 
 
 // Loads of the (immutable) matrix.  A matrix larger than L2 is streamed evict-first, so that the
 // gathered vector keeps its place in the caches; a smaller one stays cached for the next iteration.
-template <typename T>
-NGS_DEV T ld_mat(const T* p, bool stream) { return stream ? __ldcs(p) : __ldg(p); }
-
+template <bool STREAM, typename T>
+NGS_DEV T ld_mat(const T* p) {
+  if constexpr (STREAM) return __ldcs(p);
+  else return __ldg(p);
+}
 
 // y = A v over rows [row0, row1): eight lanes per row.  epi(row, acc, pre(row)) consumes each
 // row's product (lane 0 of its group) and returns a contribution to the thread's partial sum.
 // The gathered vector is read with plain loads: it was written earlier in this launch.  Ends with a
 // block barrier, after which every thread may read the rows written by the epilogue.
-template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
-NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
-                       Pre pre, Epi epi, double& dsum) {
+template <bool STREAM, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
+NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
+                         Pre pre, Epi epi, double& dsum) {
   constexpr int L = PCG_ROW_LANES;
   const int sub = threadIdx.x & (L - 1);
   const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
@@ -148,8 +150,8 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
 #pragma unroll
       for (int k = 0; k < U; k++) {
         const int64_t j = j0 + (int64_t)k * L;
-        c[k] = j < e1 ? ld_mat(a.cols + j, a.evict_first) : -1;
-        m[k] = j < e1 ? ld_mat(vals + j, a.evict_first) : (MT)0;
+        c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : -1;
+        m[k] = j < e1 ? ld_mat<STREAM>(vals + j) : (MT)0;
       }
       VT xv[U];
 #pragma unroll
@@ -171,6 +173,14 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
   }
   // the epilogue wrote rows that other threads of the block read next (their rows in phase A)
   __syncthreads();
+}
+// The streaming choice is a template argument: one load form per instantiation (a runtime choice
+// per load cost 7 % of the level-0 solve and forced register spills).
+template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
+NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
+                       Pre pre, Epi epi, double& dsum) {
+  if (a.evict_first) spmv_rows_t<true, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+  else spmv_rows_t<false, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
 }
 
 // Grid synchronisation of a cooperative launch through one arrival counter in global memory (zeroed
