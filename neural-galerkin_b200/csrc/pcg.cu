@@ -147,15 +147,17 @@ NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT
     for (int64_t j0 = e0 + sub; j0 < e1; j0 += U * L) {
       int32_t c[U];
       MT m[U];
+      // entries past the row's end gather the row's own element (cached: the diagonal's) and weigh
+      // it by zero, so that the gathers need no predicate
 #pragma unroll
       for (int k = 0; k < U; k++) {
         const int64_t j = j0 + (int64_t)k * L;
-        c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : -1;
+        c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : (int32_t)row;
         m[k] = j < e1 ? ld_mat<STREAM>(vals + j) : (MT)0;
       }
       VT xv[U];
 #pragma unroll
-      for (int k = 0; k < U; k++) xv[k] = c[k] >= 0 ? v[c[k]] : (VT)0;
+      for (int k = 0; k < U; k++) xv[k] = v[c[k]];
       // the round's products summed in the matrix type (two chains), the round sum accumulated in ACC:
       // one conversion per round instead of two per product; the FP64 refinement of the mixed mode
       // works from the true residual, so this rounding only shapes the inner iterations
