@@ -185,14 +185,20 @@ int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n, const floa
                     const int64_t* rowptr, double scale, double* vals, ngs_stream s);
 /* ngs_screen_gram with the points grouped by cell: order = the point ids sorted by keys (keys[i] is
  * the key of point order[i]: first present row of the point's 27 * 27 + that row's position, or -1
- * for a point with no voxel at this level).  One atomic per (cell, row, column) instead of per point;
- * the same sums up to the order of FP64 additions.  No counterpart in the reference. */
+ * for a point with no voxel at this level).  One atomic per (cell chunk of at most 128 points, row,
+ * column) instead of per point; the same sums up to the order of FP64 additions.  No counterpart in
+ * the reference. */
 int ngs_screen_gram_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w, const int64_t* order,
                             const int64_t* keys, const uint32_t* masks, const int64_t* rowptr, double scale,
                             double* vals, ngs_stream s);
 /* rhs[row] += scale * sum_p w[p] * phi[p,k]  (screening target term). */
 int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, const float* w, double scale, double* rhs,
                    ngs_stream s);
+/* rhs[row] += scale * sum_p w[p] * phi[p,k] * field[p] (field nullable: 1) with the points grouped
+ * by cell as for ngs_screen_gram_grouped (order / keys): one atomic per (cell chunk, row).  Covers
+ * ngs_screen_rhs (field NULL) and ngs_correction_screen (field given, scale negated). */
+int ngs_screen_rhs_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w, const float* field,
+                           const int64_t* order, const int64_t* keys, double scale, double* rhs, ngs_stream s);
 /* Divergence RHS from splatted normals of a data level (ref: reconstructor.py:126-141):
  * rhs[t] -= int grad B_t . n_data over the pairs of get_neighbours(data, target, 3).
  * tab_f / tab_g: per-axis 1-D tables (FP64) of the level ratio (see jspsr/bases/tables.py). */

@@ -162,11 +162,22 @@ extern "C" int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n,
   return NGS_OK;
 }
 
+// Points sorted by cell key are taken in chunks: a run of equal keys is cut at every multiple of
+// NGS_GROUP_CHUNK positions, so that one warp never walks more than that many points (on a coarse
+// level of a large scene, millions of points share one cell).  A chunk starts where the key changes
+// or at a cut; keys < 0 (no voxel) start nothing.
+constexpr int64_t NGS_GROUP_CHUNK = 128;
+NGS_DEV bool group_chunk_start(const int64_t* __restrict__ keys, int64_t i) {
+  const int64_t key = keys[i];
+  if (key < 0) return false;
+  return i == 0 || keys[i - 1] != key || i % NGS_GROUP_CHUNK == 0;
+}
+
 // The same sum with the points grouped by their 27-voxel neighbourhood: points in one cell share all
 // 27 rows, so their outer products are summed in registers (lane a keeps row a's 27 sums) and each
-// (row, column) slot takes one atomic per cell instead of one per point.  order / keys: the points
-// sorted by key = first present row * 27 + its position (-1: no voxel), a key that fixes the cell.
-// One warp per sorted position; the warp at the first position of a run of equal keys does the run.
+// (row, column) slot takes one atomic per cell chunk instead of one per point.  order / keys: the
+// points sorted by key = first present row * 27 + its position (-1: no voxel), a key that fixes the
+// cell.  One warp per sorted position; the warp at a chunk start does the chunk.
 __global__ void screen_gram_grouped_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi,
                                            int64_t n, const float* __restrict__ w, const int64_t* __restrict__ order,
                                            const int64_t* __restrict__ keys, const uint4* __restrict__ masks,
@@ -176,13 +187,13 @@ __global__ void screen_gram_grouped_kernel(const int32_t* __restrict__ rows, con
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = ngs_gtid() >> 5; i < n; i += warps) {
     const int64_t key = keys[i];
-    if (key < 0 || (i > 0 && keys[i - 1] == key)) continue;      // warp-uniform
+    if (!group_chunk_start(keys, i)) continue;                    // warp-uniform
     const int64_t p0 = order[i];
     const int32_t ra = lane < 27 ? rows[p0 * 27 + lane] : -1;
     double acc[27];
 #pragma unroll
     for (int b = 0; b < 27; b++) acc[b] = 0.0;
-    for (int64_t j = i; j < n && keys[j] == key; j++) {
+    for (int64_t j = i; j < n && keys[j] == key && (j == i || j % NGS_GROUP_CHUNK != 0); j++) {
       const int64_t p = order[j];
       const float pa = lane < 27 ? phi[p * 27 + lane] : 0.f;
       const double sa = (double)(w ? w[p] : 1.f) * (double)pa;
@@ -229,6 +240,44 @@ __global__ void screen_rhs_kernel(const int32_t* __restrict__ rows, const float*
   }
 }
 
+// Screening RHS terms grouped like the Gram: lane a sums w phi_a (times field, when given) over a
+// chunk of points of one cell and adds it to row a with one atomic per chunk, instead of one per
+// point (on coarse levels most points share few rows, and per-point atomics serialise there).
+__global__ void screen_rhs_grouped_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi, int64_t n,
+                                          const float* __restrict__ w, const float* __restrict__ field,
+                                          const int64_t* __restrict__ order, const int64_t* __restrict__ keys,
+                                          double scale, double* __restrict__ rhs) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ngs_gtid() >> 5; i < n; i += warps) {
+    const int64_t key = keys[i];
+    if (!group_chunk_start(keys, i)) continue;                    // warp-uniform
+    const int32_t r = lane < 27 ? rows[order[i] * 27 + lane] : -1;
+    double acc = 0.0;
+    for (int64_t j = i; j < n && keys[j] == key && (j == i || j % NGS_GROUP_CHUNK != 0); j++) {
+      const int64_t p = order[j];
+      if (lane < 27) {
+        double v = (double)phi[p * 27 + lane];
+        if (w) v *= (double)w[p];
+        if (field) v *= (double)field[p];
+        acc += v;
+      }
+    }
+    if (r >= 0) atomicAdd(rhs + r, scale * acc);
+  }
+}
+
+extern "C" int ngs_screen_rhs_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w,
+                                      const float* field, const int64_t* order, const int64_t* keys, double scale,
+                                      double* rhs, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !phi || !order || !keys || !rhs))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  { ngs_count_launch(); screen_rhs_grouped_kernel<<<ngs_blocks(n * 32, 256), 256, 0, (cudaStream_t)s>>>(
+      rows, phi, n, w, field, order, keys, scale, rhs); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
 extern "C" int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, const float* w, double scale,
                               double* rhs, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rows || !phi || !rhs))) return NGS_ERR_INVALID_ARG;
@@ -254,19 +303,34 @@ __global__ void rhs_scatter_kernel(const int32_t* __restrict__ dc, int64_t nd, i
                                    ngs_grid tg, const double* __restrict__ tc, const double* __restrict__ tgv,
                                    int tab_len, double* __restrict__ rhs) {
   const int st = tg.stride, M = st / sd;
-  for (int64_t i = ngs_gtid(); i < nd; i += ngs_gstride()) {
+  const int lane = threadIdx.x & 31;
+  // whole warps run the loop (the warp collectives below): lanes past the end contribute nothing
+  const int64_t nd_round = (nd + 31) & ~(int64_t)31;
+  for (int64_t i = ngs_gtid(); i < nd_round; i += ngs_gstride()) {
+    const bool valid = i < nd;
+    const int64_t ii = valid ? i : nd - 1;
     int q[3], c[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      c[a] = dc[i * 3 + a];
+      c[a] = dc[ii * 3 + a];
       q[a] = (int)floorf(((float)c[a] + 0.5f * (float)sd) / (float)st) * st;
     }
-    const double n0 = nrm[i * 3], n1 = nrm[i * 3 + 1], n2 = nrm[i * 3 + 2];
+    const double n0 = valid ? nrm[ii * 3] : 0.0, n1 = valid ? nrm[ii * 3 + 1] : 0.0, n2 = valid ? nrm[ii * 3 + 2] : 0.0;
+    // data voxels in lexicographic order: neighbouring lanes often share the target cell q (always,
+    // for a coarse target level).  Lanes of one run of equal q are summed by a segmented scan and
+    // the run's last lane adds the sum -- one atomic per run and target instead of one per voxel.
+    bool same_prev = true, same_next = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      same_prev &= __shfl_up_sync(0xffffffffu, q[a], 1) == q[a];
+      same_next &= __shfl_down_sync(0xffffffffu, q[a], 1) == q[a];
+    }
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || !same_prev);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));      // first lane of my run
+    const bool tail = lane == 31 || !same_next;
     for (int kx = -1; kx <= 1; kx++)
       for (int ky = -1; ky <= 1; ky++)
         for (int kz = -1; kz <= 1; kz++) {
-          const int64_t t = grid_row(tg, q[0] + kx * st, q[1] + ky * st, q[2] + kz * st);
-          if (t < 0) continue;
           const int k[3] = {kx, ky, kz};
           double cv[3], gv[3];
           bool ok = true;
@@ -278,9 +342,15 @@ __global__ void rhs_scatter_kernel(const int32_t* __restrict__ dc, int64_t nd, i
             cv[a] = ok ? tc[idx] : 0.0;
             gv[a] = ok ? tgv[idx] : 0.0;
           }
-          if (!ok) continue;
-          const double v = n0 * gv[0] * cv[1] * cv[2] + n1 * cv[0] * gv[1] * cv[2] + n2 * cv[0] * cv[1] * gv[2];
-          atomicAdd(rhs + t, -v);
+          double v = ok ? n0 * gv[0] * cv[1] * cv[2] + n1 * cv[0] * gv[1] * cv[2] + n2 * cv[0] * cv[1] * gv[2] : 0.0;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane - o >= start) v += y;
+          }
+          if (!tail) continue;
+          const int64_t t = grid_row(tg, q[0] + kx * st, q[1] + ky * st, q[2] + kz * st);
+          if (t >= 0 && v != 0.0) atomicAdd(rhs + t, -v);
         }
   }
 }

@@ -90,6 +90,7 @@ _SIGS = {
     "ngs_screen_gram": ([vp, vp, i64, vp, vp, vp, f64, vp, vp], C.c_int),
     "ngs_screen_gram_grouped": ([vp, vp, i64, vp, vp, vp, vp, vp, f64, vp, vp], C.c_int),
     "ngs_screen_rhs": ([vp, vp, i64, vp, f64, vp, vp], C.c_int),
+    "ngs_screen_rhs_grouped": ([vp, vp, i64, vp, vp, vp, vp, f64, vp, vp], C.c_int),
     "ngs_rhs_normals": ([G, vp, i64, vp, G, vp, i64, vp, vp, C.c_int, vp, vp], C.c_int),
     "ngs_correction_stiffness": ([vp, i64, C.c_int, G, vp, vp, vp, C.c_int, vp, vp], C.c_int),
     "ngs_correction_screen": ([vp, vp, i64, vp, vp, f64, vp, vp], C.c_int),

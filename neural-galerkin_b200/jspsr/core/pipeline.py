@@ -99,6 +99,7 @@ class Level:
     nnz: int = 0
     rows: torch.Tensor = None      # point basis [N, 27]
     phi: torch.Tensor = None
+    group: tuple = None            # (sorted cell keys, point order) of the screening terms
     normals: torch.Tensor = None   # splatted normal data (points with this exact level)
     rhs: torch.Tensor = None
     x64: torch.Tensor = None
@@ -266,6 +267,7 @@ class Reconstruction:
                 key = lv.rows.gather(1, first[:, None]).squeeze(1).long() * 27 + first
                 key = torch.where(present.any(1), key, torch.full_like(key, -1))
                 keys, order = torch.sort(key)
+                lv.group = (keys, order)          # reused by the screening RHS terms of this level
                 L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(order),
                        L.ptr(keys), L.ptr(lv.masks), L.ptr(lv.rowptr), sf * self.alpha, L.ptr(lv.vals64), st)
             lv.vals32 = torch.empty(lv.nnz, dtype=torch.float32, device=self.dev)
@@ -291,8 +293,9 @@ class Reconstruction:
                    lv.n, L.ptr(tc), L.ptr(tg), tc.numel(), L.ptr(rhs), st)
         sf = 0.25 ** d
         if self.alpha > 0:
-            L.call("ngs_screen_rhs", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, sf * self.alpha * self.delta,
-                   L.ptr(rhs), st)
+            keys, order = lv.group
+            L.call("ngs_screen_rhs_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, None, L.ptr(order),
+                   L.ptr(keys), sf * self.alpha * self.delta, L.ptr(rhs), st)
         coarser = list(range(self.depth - 1, d, -1))
         if coarser:
             if self.alpha > 0:
@@ -300,8 +303,9 @@ class Reconstruction:
                 for dd in coarser:
                     lc = self.levels[dd]
                     L.call("ngs_point_field", L.ptr(lc.rows), L.ptr(lc.phi), self.n, L.ptr(lc.x32), L.ptr(fieldp), 1, st)
-                L.call("ngs_correction_screen", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(fieldp),
-                       sf * self.alpha, L.ptr(rhs), st)
+                keys, order = lv.group
+                L.call("ngs_screen_rhs_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(fieldp),
+                       L.ptr(order), L.ptr(keys), -sf * self.alpha, L.ptr(rhs), st)
             for dd in coarser:
                 lc = self.levels[dd]
                 tc = L.device_table(("corr_c", lv.stride, lc.stride),
