@@ -195,8 +195,9 @@ int ngs_screen_gram_grouped(const int32_t* rows, const float* phi, int64_t n, co
 int ngs_screen_rhs(const int32_t* rows, const float* phi, int64_t n, const float* w, double scale, double* rhs,
                    ngs_stream s);
 /* rhs[row] += scale * sum_p w[p] * phi[p,k] * field[p] (field nullable: 1) with the points grouped
- * by cell as for ngs_screen_gram_grouped (order / keys): one atomic per (cell chunk, row).  Covers
- * ngs_screen_rhs (field NULL) and ngs_correction_screen (field given, scale negated). */
+ * by cell as for ngs_screen_gram_grouped (order / keys): one atomic per (run of a cell's points
+ * within 32 sorted positions, row).  Covers ngs_screen_rhs (field NULL) and ngs_correction_screen
+ * (field given, scale negated). */
 int ngs_screen_rhs_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w, const float* field,
                            const int64_t* order, const int64_t* keys, double scale, double* rhs, ngs_stream s);
 /* Divergence RHS from splatted normals of a data level (ref: reconstructor.py:126-141):

@@ -240,30 +240,40 @@ __global__ void screen_rhs_kernel(const int32_t* __restrict__ rows, const float*
   }
 }
 
-// Screening RHS terms grouped like the Gram: lane a sums w phi_a (times field, when given) over a
-// chunk of points of one cell and adds it to row a with one atomic per chunk, instead of one per
-// point (on coarse levels most points share few rows, and per-point atomics serialise there).
+// Screening RHS terms over the points sorted by cell key (the Gram's order / keys): one point per
+// lane, 32 sorted points per warp step.  For each of the 27 neighbours, the lanes of a run of equal
+// keys (points of one cell, which share their 27 rows) are summed by a segmented warp scan and the
+// run's last lane adds the sum -- one atomic per (run, row) instead of one per point.  On coarse
+// levels most points share few rows, and per-point atomics serialise there.
 __global__ void screen_rhs_grouped_kernel(const int32_t* __restrict__ rows, const float* __restrict__ phi, int64_t n,
                                           const float* __restrict__ w, const float* __restrict__ field,
                                           const int64_t* __restrict__ order, const int64_t* __restrict__ keys,
                                           double scale, double* __restrict__ rhs) {
   const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = ngs_gtid() >> 5; i < n; i += warps) {
-    const int64_t key = keys[i];
-    if (!group_chunk_start(keys, i)) continue;                    // warp-uniform
-    const int32_t r = lane < 27 ? rows[order[i] * 27 + lane] : -1;
-    double acc = 0.0;
-    for (int64_t j = i; j < n && keys[j] == key && (j == i || j % NGS_GROUP_CHUNK != 0); j++) {
-      const int64_t p = order[j];
-      if (lane < 27) {
-        double v = (double)phi[p * 27 + lane];
-        if (w) v *= (double)w[p];
-        if (field) v *= (double)field[p];
-        acc += v;
+  const int64_t n_round = (n + 31) & ~(int64_t)31;
+  for (int64_t i = ngs_gtid(); i < n_round; i += ngs_gstride()) {
+    const int64_t key = i < n ? keys[i] : -1;
+    const bool valid = key >= 0;
+    const int64_t p = valid ? order[i] : 0;
+    double sp = valid ? scale : 0.0;
+    if (valid && w) sp *= (double)w[p];
+    if (valid && field) sp *= (double)field[p];
+    const int64_t prev = __shfl_up_sync(0xffffffffu, key, 1), next = __shfl_down_sync(0xffffffffu, key, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+    const bool tail = lane == 31 || next != key;
+    for (int a = 0; a < 27; a++) {
+      double v = valid ? sp * (double)phi[p * 27 + a] : 0.0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane - o >= start) v += y;
+      }
+      if (tail && valid) {
+        const int32_t r = rows[p * 27 + a];
+        if (r >= 0) atomicAdd(rhs + r, v);
       }
     }
-    if (r >= 0) atomicAdd(rhs + r, scale * acc);
   }
 }
 
@@ -272,7 +282,7 @@ extern "C" int ngs_screen_rhs_grouped(const int32_t* rows, const float* phi, int
                                       double* rhs, ngs_stream s) {
   if (n < 0 || (n > 0 && (!rows || !phi || !order || !keys || !rhs))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;
-  { ngs_count_launch(); screen_rhs_grouped_kernel<<<ngs_blocks(n * 32, 256), 256, 0, (cudaStream_t)s>>>(
+  { ngs_count_launch(); screen_rhs_grouped_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(
       rows, phi, n, w, field, order, keys, scale, rhs); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
