@@ -188,6 +188,9 @@ int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n, const floa
  * for a point with no voxel at this level).  One atomic per (cell chunk of at most 128 points, row,
  * column) instead of per point; the same sums up to the order of FP64 additions.  No counterpart in
  * the reference. */
+/* keys[p] = first present row of rows[p, 0..26] * 27 + its position, or -1 (the cell key of
+ * ngs_screen_gram_grouped). */
+int ngs_point_cell_keys(const int32_t* rows, int64_t n, int64_t* keys, ngs_stream s);
 int ngs_screen_gram_grouped(const int32_t* rows, const float* phi, int64_t n, const float* w, const int64_t* order,
                             const int64_t* keys, const uint32_t* masks, const int64_t* rowptr, double scale,
                             double* vals, ngs_stream s);

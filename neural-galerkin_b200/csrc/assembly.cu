@@ -162,6 +162,31 @@ extern "C" int ngs_screen_gram(const int32_t* rows, const float* phi, int64_t n,
   return NGS_OK;
 }
 
+// The cell key of each point: its first present neighbour row * 27 + that neighbour's position, or
+// -1 when none of the 27 is present.  Points in one cell share all 27 rows, so the key identifies
+// the cell (the cell is the first present neighbour's voxel minus that position's offset).
+__global__ void point_cell_keys_kernel(const int32_t* __restrict__ rows, int64_t n, int64_t* __restrict__ keys) {
+  for (int64_t p = ngs_gtid(); p < n; p += ngs_gstride()) {
+    int64_t key = -1;
+    for (int a = 0; a < 27; a++) {
+      const int32_t r = rows[p * 27 + a];
+      if (r >= 0) {
+        key = (int64_t)r * 27 + a;
+        break;
+      }
+    }
+    keys[p] = key;
+  }
+}
+
+extern "C" int ngs_point_cell_keys(const int32_t* rows, int64_t n, int64_t* keys, ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rows || !keys))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  { ngs_count_launch(); point_cell_keys_kernel<<<ngs_blocks(n, 256), 256, 0, (cudaStream_t)s>>>(rows, n, keys); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
 // Points sorted by cell key are taken in chunks: a run of equal keys is cut at every multiple of
 // NGS_GROUP_CHUNK positions, so that one warp never walks more than that many points (on a coarse
 // level of a large scene, millions of points share one cell).  A chunk starts where the key changes

@@ -88,6 +88,7 @@ _SIGS = {
     "ngs_stencil_count": ([G, vp, i64, vp, vp, vp], C.c_int),
     "ngs_stencil_fill": ([G, vp, i64, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "ngs_screen_gram": ([vp, vp, i64, vp, vp, vp, f64, vp, vp], C.c_int),
+    "ngs_point_cell_keys": ([vp, i64, vp, vp], C.c_int),
     "ngs_screen_gram_grouped": ([vp, vp, i64, vp, vp, vp, vp, vp, f64, vp, vp], C.c_int),
     "ngs_screen_rhs": ([vp, vp, i64, vp, f64, vp, vp], C.c_int),
     "ngs_screen_rhs_grouped": ([vp, vp, i64, vp, vp, vp, vp, f64, vp, vp], C.c_int),

@@ -262,10 +262,8 @@ class Reconstruction:
             if self.alpha > 0:
                 sf = 0.25 ** d
                 # group the points by cell: one atomic per (cell, slot) instead of per point
-                present = lv.rows >= 0
-                first = present.to(torch.int8).argmax(1)
-                key = lv.rows.gather(1, first[:, None]).squeeze(1).long() * 27 + first
-                key = torch.where(present.any(1), key, torch.full_like(key, -1))
+                key = torch.empty(self.n, dtype=torch.int64, device=self.dev)
+                L.call("ngs_point_cell_keys", L.ptr(lv.rows), self.n, L.ptr(key), st)
                 keys, order = torch.sort(key)
                 lv.group = (keys, order)          # reused by the screening RHS terms of this level
                 L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(order),
@@ -534,10 +532,13 @@ class Reconstruction:
         # many levels the coarse boxes would make the bitmap far larger than the surface needs)
         ext = []
         for d in range(max_depth):
-            c = epb[starts[d]:starts[d] + counts[d]]
             if counts[d] == 0:
                 continue
-            ext.append(torch.cat([c.min(0).values.long(), c.max(0).values.long() + self.levels[d].stride]))
+            # the expanded cells of level d span base * n_up .. base * n_up + (n_up - 1) * stride, and
+            # their corners one stride further: the extent follows from the (n_up^3 times fewer) cells
+            c = base[d]
+            s = self.levels[d].stride
+            ext.append(torch.cat([c.min(0).values.long() * n_upsample, c.max(0).values.long() * n_upsample + n_upsample * s]))
         ext = torch.stack(ext).cpu().numpy()
         lo = ext[:, :3].min(0)
         hi = ext[:, 3:].max(0)

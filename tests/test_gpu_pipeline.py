@@ -120,6 +120,37 @@ def test_cell_field_matches_point_field(gpu_runs, name):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_grouped_screening_terms(gpu_runs, name):
+    """Cell keys from the kernel equal the torch formula; the screening RHS summed per run of a cell's
+    points (segmented warp scans) equals the per-point atomics up to FP64 summation order."""
+    from jspsr import _lib as L
+    rec = gpu_runs[name][0]
+    assert rec.alpha > 0
+    for lv in rec.levels:
+        present = lv.rows >= 0
+        first = present.to(torch.int8).argmax(1)
+        ref = lv.rows.gather(1, first[:, None]).squeeze(1).long() * 27 + first
+        ref = torch.where(present.any(1), ref, torch.full_like(ref, -1))
+        keys = torch.empty_like(ref)
+        L.call("ngs_point_cell_keys", L.ptr(lv.rows), rec.n, L.ptr(keys), L.stream())
+        assert torch.equal(keys, ref)
+        skeys, order = lv.group
+        field = torch.rand(rec.n, device=lv.rows.device)
+        for f in (None, field):
+            a = torch.zeros(lv.n, dtype=torch.float64, device=lv.rows.device)
+            b = torch.zeros_like(a)
+            if f is None:
+                L.call("ngs_screen_rhs", L.ptr(lv.rows), L.ptr(lv.phi), rec.n, None, 0.75, L.ptr(a), L.stream())
+            else:
+                L.call("ngs_correction_screen", L.ptr(lv.rows), L.ptr(lv.phi), rec.n, None, L.ptr(f), 0.75, L.ptr(a),
+                       L.stream())
+            L.call("ngs_screen_rhs_grouped", L.ptr(lv.rows), L.ptr(lv.phi), rec.n, None,
+                   L.ptr(f) if f is not None else None, L.ptr(order), L.ptr(skeys), 0.75 if f is None else -0.75,
+                   L.ptr(b), L.stream())
+            assert rel(b.cpu().numpy(), a.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_mesh_matches_oracle(cases, gpu_runs, name):
     g, _, mesh = cases[name]
     rec, v, f = gpu_runs[name]
