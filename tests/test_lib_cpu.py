@@ -24,6 +24,30 @@ def test_binding_covers_header():
     assert set(header_symbols()) == set(_lib.exported_symbols())
 
 
+def header_arities():
+    """Number of parameters of every function the header declares (comments stripped)."""
+    text = (ROOT / "include" / "ngs.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    out = {}
+    for m in re.finditer(r"\b(ngs_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_binding_arities_match_header():
+    """The ctypes prototypes take as many arguments as the C declarations (an ABI change that the
+    binding missed would pass garbage silently)."""
+    from jspsr import _lib
+    arity = header_arities()
+    wrong = {name: (len(sig[0]), arity[name]) for name, sig in _lib._SIGS.items()
+             if name in arity and len(sig[0]) != arity[name]}
+    assert not wrong, wrong
+    unchecked = set(_lib._SIGS) - set(arity)
+    assert not unchecked, unchecked
+
+
 def test_status_strings():
     from jspsr import _lib
     lib = _lib.load()
