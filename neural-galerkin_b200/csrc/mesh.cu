@@ -315,6 +315,10 @@ __global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int W, const i
                                  const int64_t* __restrict__ voff, float* __restrict__ tris,
                                  int32_t* __restrict__ vids) {
   for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
+    // voff is the exclusive scan of the count pass: a cube without vertices (most of them) is
+    // recognised from two neighbouring offsets, without reading its corners
+    const int64_t base = voff[c];
+    if (c + 1 < m && voff[c + 1] == base) continue;
     if (cnt && cnt[c] != 8) continue;
     int id[8];
     float v[8];
@@ -324,7 +328,6 @@ __global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int W, const i
       v[i] = values[id[i]];
     }
     const int t = cube_type(v);
-    const int64_t base = voff[c];
     for (int k = 0; k < 16 && c_tri[t][k] >= 0; k++) {
       const int e = c_tri[t][k];
       const int a = c_edge[e][0], b = c_edge[e][1];
