@@ -294,9 +294,11 @@ int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items, ngs_stream
 /* ngs_pcg_solve without any workspace from the caller, for callers that cannot allocate device
  * memory when they solve (no counterpart in the reference).  Scratch lives in a static device
  * array inside the library, sized for n <= ngs_pcg_noalloc_max_rows() (131072) rows; larger
- * systems return NGS_ERR_OOM before anything is launched.  The first call on each device looks
- * up the array's device address (cudaGetSymbolAddress) -- make that first call before any stream
- * capture.  All calls in the process share the one array: calls that may overlap on the GPU
+ * systems return NGS_ERR_OOM before anything is launched, a negative n NGS_ERR_INVALID_ARG.  Every
+ * call looks up the array's device address in the CUDA context current at the call
+ * (cudaGetSymbolAddress; it allocates nothing), so primary and driver-created contexts alike get
+ * their own copy; the first call in each context loads the library's device code there -- make
+ * that first call before any stream capture.  All calls in the process share the one array: calls that may overlap on the GPU
  * (different streams, or concurrent host threads) race and must be serialised by the caller.
  * Nothing is allocated: no cudaMalloc / cudaFree, no allocating library routine. */
 int64_t ngs_pcg_noalloc_max_rows(void);

@@ -28,7 +28,10 @@ def parse_tri_table(header_text: str):
 
 def main(src: str):
     rows = parse_tri_table(Path(src).read_text())
-    lines = ["/* Marching-cubes triangle table (Lorensen/Bourke), 256 x 16, -1 terminated. Data only. */"]
+    lines = ["/* Marching-cubes triangle table (Lorensen/Bourke), 256 x 16, -1 terminated. Data only.",
+             " * Taken as data from huangjh-pub/neural-galerkin csrc/marching_cubes/mc_data.cuh,",
+             " * Copyright 2022 Jiahui Huang, Hao-Xiang Chen, Shi-Min Hu, MIT licence (permission notice:",
+             " * the LICENSE file of that project); table originally published by Paul Bourke. */"]
     lines += ["{" + ", ".join(f"{v:2d}" for v in r) + "}," for r in rows]
     OUT.write_text("\n".join(lines) + "\n")
 

@@ -552,7 +552,7 @@ extern "C" int ngs_vdedup_sort(const int32_t* vert_ids, int64_t n_keys, const in
   cudaStream_t st = (cudaStream_t)s;
   { ngs_count_launch(); vd_scatter_kernel<<<ngs_blocks(n_keys, 256), 256, 0, st>>>(vert_ids, n_keys, bucket_start, bucket_fill, sorted_keys); }
   { ngs_count_launch(); vd_sort_kernel<<<ngs_blocks(n_buckets, 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
-  { ngs_count_launch(); vd_sort_big_kernel<<<(unsigned)std::min<int64_t>(148 * 8, (n_buckets + 255) / 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
+  { ngs_count_launch(); vd_sort_big_kernel<<<(unsigned)std::min<int64_t>((int64_t)ngs_num_sms() * 8, (n_buckets + 255) / 256), 256, 0, st>>>(bucket_start, bucket_fill, n_buckets, sorted_keys, first); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

@@ -148,8 +148,13 @@ void ngs_count_launch();
 NGS_DEV int64_t ngs_gtid() { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
 NGS_DEV int64_t ngs_gstride() { return (int64_t)gridDim.x * blockDim.x; }
 
-inline unsigned int ngs_blocks(int64_t n, int threads, int64_t cap = 148 * 64) {
+// Streaming multiprocessors of the current device (queried once per device and cached).
+int ngs_num_sms();
+
+// Grid of a grid-stride kernel: enough blocks for n items, at most per_sm blocks per SM.
+inline unsigned int ngs_blocks(int64_t n, int threads, int per_sm = 64) {
   int64_t b = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)ngs_num_sms() * per_sm;
   if (b < 1) b = 1;
   if (b > cap) b = cap;
   return (unsigned int)b;

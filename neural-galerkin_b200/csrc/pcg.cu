@@ -35,7 +35,6 @@
 // into the single-system and the batched kernel, and only uncontracted arithmetic is guaranteed to
 // round the same way in both, which makes a batched solve bit-identical to the solo one.
 #include <cmath>
-#include <mutex>
 #include "ngs_common.cuh"
 
 constexpr int PCG_THREADS = 512;
@@ -45,6 +44,11 @@ constexpr int PCG_ROW_COST = 8;        // work of a row on top of its non-zeros 
 constexpr int PCG_BLOCK_WORK = 16384;  // work (non-zeros + row cost) that justifies one more block
 constexpr int PCG_CLUSTER_MAX = 16;    // CTAs of the largest thread-block cluster a small system gets
 constexpr int PCG_CLUSTER_NEED = 64;   // systems of at most this many blocks' work are solved by a cluster
+// Most blocks one cooperative solve may use (B200: 148 SMs x 2 = 296).  The capacity query clamps to
+// it, and the per-block partials area of the workspace is sized from it: reductions double-buffer the
+// partials by barrier parity, 2 x PCG_MAX_BLOCKS x 4 doubles.
+constexpr int PCG_MAX_BLOCKS = 1024;
+constexpr size_t PCG_PARTIALS_BYTES = (size_t)2 * PCG_MAX_BLOCKS * 4 * sizeof(double);
 
 struct PcgArgs {
   int64_t n;
@@ -369,6 +373,23 @@ template <> struct PcgTypes<NGS_PCG_REFERENCE> { using MT = float; using VT = fl
 template <> struct PcgTypes<NGS_PCG_MIXED> { using MT = float; using VT = float; using RT = double; using ACC = double; };
 template <> struct PcgTypes<NGS_PCG_FP64> { using MT = double; using VT = double; using RT = double; using ACC = double; };
 
+// Status of a solve.  The launcher zeroes info; every write is a maximum, and the codes grow with
+// severity (OK < INVALID_ARG < NOT_CONVERGED < TIMEOUT), so that a block that gave up at a barrier
+// and block 0 finishing its own rows can both write without one hiding the other.
+NGS_DEV void pcg_record(const PcgArgs& a, int status, int it) {
+  atomicMax(reinterpret_cast<unsigned long long*>(a.info + 1), (unsigned long long)status);
+  atomicMax(reinterpret_cast<unsigned long long*>(a.info), (unsigned long long)it);
+}
+
+// A barrier or reduction gave up (its bounded wait ran out, or another block recorded an error):
+// the block leaves the solve and says why.
+NGS_DEV void pcg_abandon(const PcgArgs& a, int it) {
+  if (threadIdx.x == 0) {
+    const int e = *reinterpret_cast<volatile int*>(a.error);
+    pcg_record(a, e != 0 ? e : NGS_ERR_TIMEOUT, it);
+  }
+}
+
 // The solve of one system by the blocks bid = 0 .. a.nblocks-1 of a launch (all of them for a
 // single solve, a contiguous range for one system of a batch, the CTAs of one cluster).
 template <int MODE, typename Sync>
@@ -414,6 +435,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
 
   // init: x = 0, r = b, u = M r, p = s = 0; partial (b, b); part[1] flags empty rows
   double part[3] = {0.0, rows_ok ? 0.0 : 1.0, 0.0}, res[3];
+  int it = 0, replacements = 0;
   for (int64_t i = i0; i < i1; i += is) {
     const RT bi = b[i];
     x[i] = (RT)0;
@@ -423,12 +445,9 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
     s[i] = (VT)0;
     part[0] += (double)bi * (double)bi;
   }
-  if (!sy.template reduce<3>(part, res)) return;
+  if (!sy.template reduce<3>(part, res)) return pcg_abandon(a, it);
   if (res[1] > 0.0) {                                    // every block sees the same flag: no copy was issued
-    if (bid == 0 && threadIdx.x == 0) {
-      a.info[0] = 0;
-      a.info[1] = NGS_ERR_INVALID_ARG;
-    }
+    if (bid == 0 && threadIdx.x == 0) pcg_record(a, NGS_ERR_INVALID_ARG, 0);
     return;
   }
   const double bnorm = sqrt(res[0]);
@@ -439,10 +458,9 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
     part[0] += (double)r[i] * (double)u[i];
     part[2] += (double)r[i] * (double)r[i];
   }
-  if (!sy.template reduce<3>(part, res)) return;
+  if (!sy.template reduce<3>(part, res)) return pcg_abandon(a, it);
   double gamma = res[0], delta = res[1], rho = res[2];
   double alpha = delta != 0.0 ? gamma / delta : 0.0, beta = 0.0;
-  int it = 0, replacements = 0;
   const double rtol_inner = MODE == NGS_PCG_MIXED ? a.inner_rtol : 0.0;
   double target = fmax(atol, rtol_inner * sqrt(rho));
   bool converged = sqrt(rho) <= atol || bnorm == 0.0, timed_out = false;
@@ -472,17 +490,17 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
     }
     if (replace) {
       // residual replacement: r = b - A x (FP64 matrix in MIXED mode, the FP32 one in REFERENCE mode)
-      if (!sy.barrier()) return;
+      if (!sy.barrier()) return pcg_abandon(a, it);
       double rr = 0.0;
       spmv_true(rr);
       part[2] = rr;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       replacements++;
     }
-    if (!sy.barrier()) return;
+    if (!sy.barrier()) return pcg_abandon(a, it);
     // phase B: w = A u and (w, u)
     spmv_w(part[1]);
-    if (!sy.template reduce<3>(part, res)) return;
+    if (!sy.template reduce<3>(part, res)) return pcg_abandon(a, it);
     it++;
     const double gamma_new = res[0];
     delta = res[1];
@@ -490,14 +508,14 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
     if (sqrt(rho) <= target) {
       if (MODE != NGS_PCG_MIXED) { converged = true; break; }
       // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
-      if (!sy.barrier()) return;
+      if (!sy.barrier()) return pcg_abandon(a, it);
       part[0] = part[1] = part[2] = 0.0;
       spmv_true(part[2]);
       replacements++;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
-      if (!sy.barrier()) return;
+      if (!sy.barrier()) return pcg_abandon(a, it);
       spmv_w(part[1]);
-      if (!sy.template reduce<3>(part, res)) return;
+      if (!sy.template reduce<3>(part, res)) return pcg_abandon(a, it);
       rho = res[2];
       if (sqrt(rho) <= atol) { converged = true; break; }
       gamma = res[0];
@@ -515,8 +533,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   if (a.x32_out)
     for (int64_t i = i0; i < i1; i += is) a.x32_out[i] = (float)x[i];
   if (bid == 0 && threadIdx.x == 0) {
-    a.info[0] = it;
-    a.info[1] = converged ? NGS_OK : (timed_out ? NGS_ERR_TIMEOUT : NGS_ERR_NOT_CONVERGED);
+    pcg_record(a, converged ? NGS_OK : (timed_out ? NGS_ERR_TIMEOUT : NGS_ERR_NOT_CONVERGED), it);
     a.info[2] = replacements;
     a.resid[0] = sqrt(rho);
     a.resid[1] = bnorm;
@@ -571,7 +588,7 @@ extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
   const size_t vt = pcg_vec_bytes(mode);
   const size_t rt = pcg_res_bytes(mode);
   size_t bytes = align_up(n * rt) + 4 * align_up(n * vt);     // r, p, s, u, w
-  bytes += align_up((size_t)148 * 32 * 4 * sizeof(double));    // partials (upper bound of blocks)
+  bytes += align_up(PCG_PARTIALS_BYTES);                        // partials, double-buffered
   bytes += align_up(4 * sizeof(double)) + align_up(8 * sizeof(unsigned int));
   return bytes;
 }
@@ -587,7 +604,7 @@ static int pcg_capacity() {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_batch, pcg_batch_kernel<MODE>, PCG_THREADS, 0);
   if (per_sm_batch < per_sm) per_sm = per_sm_batch;
   const int64_t cap = (int64_t)sms * per_sm;
-  return (int)(cap < 148 * 32 ? cap : 148 * 32);
+  return (int)(cap < PCG_MAX_BLOCKS ? cap : PCG_MAX_BLOCKS);   // the partials area holds this many blocks
 }
 
 // Blocks one solve uses: as many co-resident blocks as fit, fewer for small systems (about
@@ -697,8 +714,15 @@ static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
   return NGS_OK;
 }
 
+// Zero a system's status record: the kernel's status writes are maxima over it, and an empty system
+// (nothing to launch) reports 0 iterations, NGS_OK.
+static void pcg_clear_status(int64_t* info_dev, double* resid_dev, cudaStream_t st) {
+  cudaMemsetAsync(info_dev, 0, 4 * sizeof(int64_t), st);
+  cudaMemsetAsync(resid_dev, 0, 2 * sizeof(double), st);
+}
+
 // Validate one system, carve its workspace and fill the kernel arguments (nblocks left 0).
-// Returns NGS_OK, an error, or 1 for an empty system (status written, nothing to launch).
+// Returns NGS_OK, an error, or 1 for an empty system (nothing to launch).  Touches no device memory.
 static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
                        int64_t* info_dev, double* resid_dev, cudaStream_t st, PcgArgs& a) {
   if (!sys || !cfg || !info_dev || !resid_dev || sys->n < 0 || !sys->rowptr || (sys->nnz > 0 && !sys->cols) ||
@@ -711,11 +735,7 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   if (mode == NGS_PCG_FP64 && (!sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
   if (!ws || ws_bytes < ngs_pcg_workspace_bytes(sys->n, mode)) return NGS_ERR_OOM;
   const int64_t n = sys->n;
-  if (n == 0) {
-    cudaMemsetAsync(info_dev, 0, 4 * sizeof(int64_t), st);
-    cudaMemsetAsync(resid_dev, 0, 2 * sizeof(double), st);
-    return 1;
-  }
+  if (n == 0) return 1;
   const size_t vt = pcg_vec_bytes(mode);
   const size_t rt = pcg_res_bytes(mode);
   char* base = static_cast<char*>(ws);
@@ -735,7 +755,7 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.s = base; base += align_up(n * vt);
   a.u = base; base += align_up(n * vt);
   a.w = base; base += align_up(n * vt);
-  a.partials = reinterpret_cast<double*>(base); base += align_up((size_t)148 * 32 * 4 * sizeof(double));
+  a.partials = reinterpret_cast<double*>(base); base += align_up(PCG_PARTIALS_BYTES);
   unsigned int* ctl = reinterpret_cast<unsigned int*>(base);
   a.count = ctl;
   a.error = reinterpret_cast<int*>(ctl + 2);
@@ -771,8 +791,9 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   cudaStream_t st = (cudaStream_t)s;
   PcgArgs a;
   const int rc = prepare_pcg(sys, cfg, ws, ws_bytes, info_dev, resid_dev, st, a);
+  if (rc != NGS_OK && rc != 1) return rc;
+  pcg_clear_status(info_dev, resid_dev, st);
   if (rc == 1) return NGS_OK;
-  if (rc != NGS_OK) return rc;
   const int csize = pcg_cluster_for(a.n, a.nnz, cfg->blocks, cluster_limit_of(cfg->mode));
   if (csize > 0) return launch_cluster(a, cfg->mode, csize, st);
   const int cap = capacity_of(cfg->mode);
@@ -802,8 +823,9 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
   static thread_local PcgBatch b;          // 15 KB: kept off the stack
   static thread_local PcgArgs small[NGS_PCG_BATCH_MAX];
   static thread_local int small_size[NGS_PCG_BATCH_MAX];
+  static thread_local int empty[NGS_PCG_BATCH_MAX];
   b.nsys = 0;
-  int nsmall = 0;
+  int nsmall = 0, nempty = 0;
   unsigned int total = 0;
   const int climit = cluster_limit_of(mode);
   // validate and size everything before the first memset, so that a rejected batch touches nothing
@@ -811,7 +833,10 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     const ngs_pcg_batch_item& it = items[k];
     PcgArgs a;
     const int rc = prepare_pcg(&it.sys, &it.cfg, it.ws, it.ws_bytes, it.info_dev, it.resid_dev, st, a);
-    if (rc == 1) continue;
+    if (rc == 1) {
+      empty[nempty++] = k;
+      continue;
+    }
     if (rc != NGS_OK) return rc;
     const int csize = pcg_cluster_for(a.n, a.nnz, it.cfg.blocks, climit);
     if (csize > 0) {                         // solved by its own cluster, as it would be alone
@@ -827,13 +852,18 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     b.sys[b.nsys++] = a;
     total += (unsigned)blocks;
   }
+  for (int k = 0; k < nempty; k++) pcg_clear_status(items[empty[k]].info_dev, items[empty[k]].resid_dev, st);
   for (int k = 0; k < nsmall; k++) {
+    pcg_clear_status(small[k].info, small[k].resid, st);
     const int rc = launch_cluster(small[k], mode, small_size[k], st);
     if (rc != NGS_OK) return rc;
   }
   if (b.nsys == 0) return NGS_OK;
   b.start[b.nsys] = total;
-  for (int k = 0; k < b.nsys; k++) cudaMemsetAsync(b.sys[k].count, 0, 8 * sizeof(unsigned int), st);
+  for (int k = 0; k < b.nsys; k++) {
+    pcg_clear_status(b.sys[k].info, b.sys[k].resid, st);
+    cudaMemsetAsync(b.sys[k].count, 0, 8 * sizeof(unsigned int), st);
+  }
   void* args[] = {&b};
   ngs_count_launch();
   const cudaError_t e = cudaLaunchCooperativeKernel(pcg_batch_kernel_of(mode), dim3(total), dim3(PCG_THREADS), args,
@@ -853,29 +883,19 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
 static constexpr int64_t kNoallocMaxRows = 131072;
 static constexpr size_t noalloc_align(size_t v) { return (v + 255) & ~(size_t)255; }
 static constexpr size_t kNoallocScratchBytes =
-    noalloc_align(kNoallocMaxRows * 8) + 4 * noalloc_align(kNoallocMaxRows * 8) +
-    noalloc_align((size_t)148 * 32 * 4 * sizeof(double)) + noalloc_align(4 * sizeof(double)) +
-    noalloc_align(8 * sizeof(unsigned int));
+    noalloc_align(kNoallocMaxRows * 8) + 4 * noalloc_align(kNoallocMaxRows * 8) + noalloc_align(PCG_PARTIALS_BYTES) +
+    noalloc_align(4 * sizeof(double)) + noalloc_align(8 * sizeof(unsigned int));
 static __device__ __align__(256) unsigned char g_pcg_noalloc_scratch[kNoallocScratchBytes];
 
-// The host cannot use g_pcg_noalloc_scratch as a device address: its device address is looked up
-// once per device (with that device current) and cached here.
-static std::mutex g_noalloc_mutex;
-static void* g_noalloc_ptr[256] = {};
-
+// The host cannot use g_pcg_noalloc_scratch as a device address.  Its address belongs to the CUDA
+// context that is current, so it is looked up on every call, with that context current (the lookup
+// allocates nothing; the first one in a context loads this library's device code into it, which is
+// why the first call in each context should come before any stream capture).
 static int noalloc_scratch(void** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_noalloc_scratch);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
-  if (dev < 0 || dev >= 256) return NGS_ERR_INVALID_ARG;
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_pcg_noalloc_scratch);
-    if (e != cudaSuccess) return ngs_set_cuda_error(e);
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
+  *out = p;
   return NGS_OK;
 }
 
@@ -883,14 +903,15 @@ extern "C" int64_t ngs_pcg_noalloc_max_rows(void) { return kNoallocMaxRows; }
 
 extern "C" int ngs_pcg_solve_noalloc(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, int64_t* info_dev,
                                      double* resid_dev, ngs_stream s) {
-  if (!sys || !cfg) return NGS_ERR_INVALID_ARG;
+  if (!sys || !cfg || sys->n < 0) return NGS_ERR_INVALID_ARG;
   if (sys->n > kNoallocMaxRows) return NGS_ERR_OOM;            // too large for the built-in scratch
   if (ngs_pcg_workspace_bytes(sys->n, cfg->mode) > kNoallocScratchBytes) return NGS_ERR_OOM;
   void* ws = nullptr;
   const int rc = noalloc_scratch(&ws);
   if (rc != NGS_OK) return rc;
-  // ngs_pcg_solve clears the control words it needs zeroed and the kernel initialises every vector,
-  // so leftovers of the previous call in the shared scratch do not matter.
+  // ngs_pcg_solve clears the control words it needs zeroed (arrival counter, error word, deadline)
+  // and the kernel initialises every vector and writes each partial before reading it, so what the
+  // previous call left in the shared scratch does not matter.
   return ngs_pcg_solve(sys, cfg, ws, kNoallocScratchBytes, info_dev, resid_dev, s);
 }
 
@@ -939,7 +960,7 @@ extern "C" int ngs_spmv64(int64_t n, const int64_t* rowptr, const int32_t* cols,
 extern "C" int ngs_dot64(const double* a, const double* b, int64_t n, double* out_dev, ngs_stream s) {
   if (n < 0 || !out_dev || (n > 0 && (!a || !b))) return NGS_ERR_INVALID_ARG;
   cudaMemsetAsync(out_dev, 0, sizeof(double), (cudaStream_t)s);
-  if (n > 0) { ngs_count_launch(); dot64_kernel<<<ngs_blocks(n, 256, 148 * 4), 256, 0, (cudaStream_t)s>>>(a, b, n, out_dev); }
+  if (n > 0) { ngs_count_launch(); dot64_kernel<<<ngs_blocks(n, 256, 4), 256, 0, (cudaStream_t)s>>>(a, b, n, out_dev); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

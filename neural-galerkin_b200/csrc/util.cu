@@ -21,6 +21,23 @@ extern "C" void ngs_reset_launch_count(void) { g_launches.store(0, std::memory_o
 
 extern "C" int ngs_version(void) { return 10000; }
 
+int ngs_num_sms() {
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  if (dev >= 0 && dev < 64) {
+    const int c = cached[dev].load(std::memory_order_relaxed);
+    if (c > 0) return c;
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+    cudaGetLastError();
+    sms = 1;
+  }
+  if (dev >= 0 && dev < 64) cached[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
+
 extern "C" const char* ngs_status_string(int status) {
   switch (status) {
     case NGS_OK: return "ok";
@@ -113,7 +130,7 @@ extern "C" int ngs_points_bbox(const float* xyz, int64_t n, float* bbox_dev, ngs
   cudaStream_t st = (cudaStream_t)s;
   unsigned int* b = reinterpret_cast<unsigned int*>(bbox_dev);
   { ngs_count_launch(); bbox_init_kernel<<<1, 32, 0, st>>>(b); }
-  { ngs_count_launch(); bbox_kernel<<<ngs_blocks(n, 256, 148 * 8), 256, 0, st>>>(xyz, n, b); }
+  { ngs_count_launch(); bbox_kernel<<<ngs_blocks(n, 256, 8), 256, 0, st>>>(xyz, n, b); }
   { ngs_count_launch(); bbox_decode_kernel<<<1, 32, 0, st>>>(b); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
@@ -140,7 +157,7 @@ extern "C" int ngs_weighted_sum(const float* v, const float* w, int64_t n, doubl
   if (n < 0 || !v || !sums_dev) return NGS_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)s;
   cudaMemsetAsync(sums_dev, 0, 2 * sizeof(double), st);
-  if (n > 0) { ngs_count_launch(); weighted_sum_kernel<<<ngs_blocks(n, 256, 148 * 4), 256, 0, st>>>(v, w, n, sums_dev); }
+  if (n > 0) { ngs_count_launch(); weighted_sum_kernel<<<ngs_blocks(n, 256, 4), 256, 0, st>>>(v, w, n, sums_dev); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

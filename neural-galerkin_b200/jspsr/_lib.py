@@ -18,7 +18,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libngs.so"
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "buffer or workspace too small", 3: "hash insert failed",
           4: "not converged", 5: "topology error", 6: "CUDA error", 7: "device-side wait timed out"}
-NGS_OK, NGS_ERR_INVALID_ARG, NGS_ERR_NOT_CONVERGED, NGS_ERR_TIMEOUT = 0, 1, 4, 7
+NGS_OK, NGS_ERR_INVALID_ARG, NGS_ERR_OOM, NGS_ERR_HASH_INSERT, NGS_ERR_NOT_CONVERGED = 0, 1, 2, 3, 4
+NGS_ERR_TOPOLOGY, NGS_ERR_CUDA, NGS_ERR_TIMEOUT = 5, 6, 7
 PCG_REFERENCE, PCG_MIXED, PCG_FP64 = 0, 1, 2
 MAX_FIELD_LEVELS = 16
 

@@ -20,6 +20,7 @@ structures are new:
 from __future__ import annotations
 
 import math
+import warnings
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -406,8 +407,10 @@ class Reconstruction:
                 break
         lv.x64 = x
         lv.x32.copy_(x)
+        res = math.sqrt(dotv(r, r))
         lv.info[0] = it
-        lv.resid[0] = math.sqrt(dotv(r, r))
+        lv.info[1] = L.NGS_OK if res <= atol else L.NGS_ERR_NOT_CONVERGED
+        lv.resid[0] = res
         lv.resid[1] = atol / spec.tol if spec.tol > 0 else 0.0
 
     def solve(self):
@@ -417,24 +420,46 @@ class Reconstruction:
             self._mark(f"rhs{d}")
             self._solve_level(self.levels[d], d)
             self._mark(f"pcg{d}")
+        self._queue_status()
         return self
+
+    def _queue_status(self):
+        """Copy every level's solve record to pinned host memory behind the solves, without waiting:
+        the mesh extraction synchronises with the device anyway, after which the copy has landed."""
+        rec = torch.cat([torch.cat([lv.info.double(), lv.resid]) for lv in self.levels])
+        self._status_host = torch.empty(rec.shape, dtype=torch.float64, pin_memory=True)
+        self._status_host.copy_(rec, non_blocking=True)
+        self._status_event = torch.cuda.Event()
+        self._status_event.record()
+
+    def check_solves(self):
+        """Iteration counts and status of every level; raises ``NgsError`` when a solve failed.
+
+        A solve that gave up (a bounded device wait ran out: NGS_ERR_TIMEOUT), was handed an invalid
+        system, or stopped at the library's own iteration cap without reaching the tolerance raises.
+        A solve that stopped at a ``maxiter`` the caller asked for keeps the reference's behaviour
+        (``solver.py:138-143``: the result is returned and the residual reported) with a warning."""
+        if getattr(self, "_status_host", None) is None:
+            self._queue_status()
+        self._status_event.synchronize()
+        rec = self._status_host.numpy().reshape(self.depth, 6)
+        self.solve_stats = {d: dict(iters=int(rec[d, 0]), status=int(rec[d, 1]), replacements=int(rec[d, 2]),
+                                    resid=float(rec[d, 4]), bnorm=float(rec[d, 5])) for d in range(self.depth)}
+        for d, s in self.solve_stats.items():
+            if s["status"] == L.NGS_OK:
+                continue
+            if s["status"] == L.NGS_ERR_NOT_CONVERGED and self.solver.maxiter >= 0:
+                warnings.warn(f"PCG level {d} stopped at maxiter={self.solver.maxiter} with residual "
+                              f"{s['resid']:.3e} (|b| = {s['bnorm']:.3e})", RuntimeWarning, stacklevel=3)
+                continue
+            raise L.NgsError(s["status"], f"PCG level {d}")
+        return self.solve_stats
 
     @property
     def pcg_ms(self):
         """Device time of each level's PCG launch (needs profile_pcg = True before solve)."""
         torch.cuda.synchronize()
         return {d: e[0].elapsed_time(e[1]) for d, e in self._pcg_events.items()}
-
-    def check_solves(self):
-        """Read back iteration counts / status of every level (one sync)."""
-        info = torch.stack([lv.info for lv in self.levels]).cpu().numpy()
-        resid = torch.stack([lv.resid for lv in self.levels]).cpu().numpy()
-        self.solve_stats = {d: dict(iters=int(info[d, 0]), status=int(info[d, 1]), replacements=int(info[d, 2]),
-                                    resid=float(resid[d, 0]), bnorm=float(resid[d, 1])) for d in range(self.depth)}
-        for d, s in self.solve_stats.items():
-            if s["status"] not in (L.NGS_OK, L.NGS_ERR_NOT_CONVERGED):
-                raise L.NgsError(s["status"], f"PCG level {d}")
-        return self.solve_stats
 
     # ------------------------------------------------------------------ field
     def chi_raw(self, pos: torch.Tensor, grad: bool = False) -> torch.Tensor:
@@ -651,4 +676,6 @@ class Reconstruction:
 
     def run(self, n_upsample: int = 2):
         self.build_tree().assemble().solve()
-        return self.extract_mesh(n_upsample)
+        mesh = self.extract_mesh(n_upsample)
+        self.check_solves()            # the mesh extraction has synchronised: no extra wait
+        return mesh

@@ -40,7 +40,11 @@ class HashLookupData:
         L.call("ngs_hash_table_build", C.byref(self.table), L.ptr(keys.contiguous().long()),
                L.ptr(vals.contiguous().long()) if use_vals else None, n, L.ptr(status), L.stream())
         self.inserted_size = n
-        self._status = status
+        # the reference synchronises after its insert and ignores a failed one
+        # (hashmap_cuda.cu:152,187,369); here the insert status is read at that sync and raised
+        rc = int(status.item())
+        if rc != L.NGS_OK:
+            raise L.NgsError(rc, "build_hash_table")
 
     def device(self):
         return self.slots.device

@@ -21,9 +21,10 @@ neighbour queries, density, levels, RHS / LHS assembly, correction, chi,
 conformal tree, dual-grid construction, vertex de-duplication) is the
 reference's own code.  The learned-basis case also writes the reference's additive-integral cache files (which it
 would otherwise compute with sympy) from its own symbolic components.  Run from the
-repository root (``python tests/golden/make_golden.py [tables|learned|<case>...]``):
+repository root, with the reference checkout named by ``NGS_REFERENCE_DIR``
+(``python tests/golden/make_golden.py [tables|learned|<case>...]``):
 
-    python tests/golden/make_golden.py
+    NGS_REFERENCE_DIR=/path/to/neural-galerkin python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -38,7 +39,8 @@ from pathlib import Path
 import numpy as np
 import torch
 
-REF = Path("/root/reference")
+# the reference checkout (huangjh-pub/neural-galerkin), named by NGS_REFERENCE_DIR
+REF = Path(os.environ.get("NGS_REFERENCE_DIR", "../neural-galerkin")).resolve()
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))

@@ -73,13 +73,20 @@ def solve(lib, L, m, b64, noalloc):
     return x64.cpu().numpy(), int(info[0])
 
 
-def test_noalloc_matches_workspace_solve_twice():
+@pytest.mark.parametrize("side", [40, 50])
+def test_noalloc_matches_workspace_solve_twice(side):
+    """side 40 (64,000 rows) is solved by one thread-block cluster, whose reductions live in
+    distributed shared memory; side 50 (125,000 rows) needs more blocks than a cluster holds and takes
+    the cooperative grid path, whose per-block partials, arrival counter, error word and deadline
+    live in the shared static scratch -- the second call runs on what the first one left there."""
     from jspsr import _lib as L
     lib = L.load()
     dev = torch.device("cuda", 0)
-    m = laplacian_system(40, 0.3, dev)                     # 64,000 rows
+    m = laplacian_system(side, 0.3, dev)
     assert m["n"] <= lib.ngs_pcg_noalloc_max_rows()
-    gen = torch.Generator(device="cpu").manual_seed(0)
+    cluster = lib.ngs_pcg_cluster_size(m["n"], m["nnz"], L.PCG_MIXED)
+    assert (cluster > 0) == (side == 40), cluster
+    gen = torch.Generator(device="cpu").manual_seed(side)
     for call in range(2):                                  # the second call runs on the first one's leftovers
         b = torch.randn(m["n"], generator=gen, dtype=torch.float64).to(dev)
         x_ref, it_ref = solve(lib, L, m, b, noalloc=False)
@@ -97,3 +104,6 @@ def test_noalloc_rejects_oversized_system():
     cfg.mode = L.PCG_MIXED
     rc = lib.ngs_pcg_solve_noalloc(C.byref(sysd), C.byref(cfg), None, None, L.stream())
     assert rc == 2                                         # NGS_ERR_OOM: larger than the built-in scratch
+    sysd.n = -1
+    rc = lib.ngs_pcg_solve_noalloc(C.byref(sysd), C.byref(cfg), None, None, L.stream())
+    assert rc == 1                                         # NGS_ERR_INVALID_ARG, as ngs_pcg_solve
