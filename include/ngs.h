@@ -105,6 +105,29 @@ typedef struct ngs_grid {
   void* words;          /* nwords x 16 bytes {uint32 rank, uint32 pad, uint64 bits}, zeroed before marking */
 } ngs_grid;
 
+/* Fused neighbour query of one level (ref: jspsr/core/_hash_backend.py:176-228, which builds the
+ * [K, N] key matrix of csrc/common/hashmap_cuda.cu:204-235, probes the level's cuckoo table and
+ * compacts with torch.where).  Two passes over tiles of 256 sources, no K x N intermediate.
+ * src: float [n,3] (src_float = 1; the reference's point queries xyz / vs - 0.5) or int32 [n,3]
+ * voxel coordinates at src_stride.  conv = 0 snaps each source to the level's lattice as
+ * floor((src + src_stride/2) / g.stride) * g.stride, conv = 1 uses it as is; the probes are
+ * origin + offsets[j] * g.stride, j < k <= 128.  row_of_rank (optional, int64 [ranks]) maps a
+ * lexicographic rank to the row of a level whose coordinate list is not sorted.
+ * transposed = 0 (k-major): tile_counts int64 [k * ngs_grid_neighbours_tiles(n)] (offset-major)
+ * and per_offset int64 [k] (the reference's nbsizes); transposed = 1 (source-major): per_source
+ * int64 [n].  masks: int32 [n, 4] scratch carried from count to fill.  start = exclusive scan of
+ * tile_counts (k-major) or per_source (source-major); fill writes int64 src_ids, int64 tgt_ids and
+ * int32 kidx (offset index) of every hit in the chosen order. */
+int64_t ngs_grid_neighbours_tiles(int64_t n);
+int ngs_grid_neighbours_count(ngs_grid g, const int64_t* row_of_rank, const void* src, int src_float, int64_t n,
+                              int src_stride, int conv, const int32_t* offsets, int k, int transposed,
+                              uint32_t* masks, int64_t* tile_counts, int64_t* per_offset, int64_t* per_source,
+                              ngs_stream s);
+int ngs_grid_neighbours_fill(ngs_grid g, const int64_t* row_of_rank, const void* src, int src_float, int64_t n,
+                             int src_stride, int conv, const int32_t* offsets, int k, int transposed,
+                             const uint32_t* masks, const int64_t* start, int64_t* src_ids, int64_t* tgt_ids,
+                             int32_t* kidx, ngs_stream s);
+
 /* min/max of a float [n,3] array -> bbox_dev float[6] = (min xyz, max xyz) */
 int ngs_points_bbox(const float* xyz, int64_t n, float* bbox_dev, ngs_stream s);
 /* Mark the 8 trilinear corner cells of every point with level <= max_level

@@ -77,6 +77,11 @@ _SIGS = {
     "ngs_grid_finalize": ([G, vp, sz, vp, vp], C.c_int),
     "ngs_grid_emit_coords": ([G, vp, vp], C.c_int),
     "ngs_grid_lookup": ([G, vp, i64, vp, vp], C.c_int),
+    "ngs_grid_neighbours_tiles": ([i64], i64),
+    "ngs_grid_neighbours_count": ([G, vp, vp, C.c_int, i64, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp,
+                                   vp, vp], C.c_int),
+    "ngs_grid_neighbours_fill": ([G, vp, vp, C.c_int, i64, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, vp,
+                                  vp, vp], C.c_int),
     "ngs_splat_weights": ([G, vp, i64, f32, f64, vp, vp], C.c_int),
     "ngs_density_eval": ([G, vp, i64, f32, f64, vp, f32, C.c_int, vp, vp, vp, vp], C.c_int),
     "ngs_splat_data": ([G, vp, i64, f32, f64, vp, C.c_int, vp, vp, C.c_int, f32, vp, vp], C.c_int),

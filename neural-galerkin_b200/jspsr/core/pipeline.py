@@ -423,9 +423,12 @@ class Reconstruction:
         self._queue_status()
         return self
 
+    _status_checked = False
+
     def _queue_status(self):
         """Copy every level's solve record to pinned host memory behind the solves, without waiting:
         the mesh extraction synchronises with the device anyway, after which the copy has landed."""
+        self._status_checked = False
         rec = torch.cat([torch.cat([lv.info.double(), lv.resid]) for lv in self.levels])
         self._status_host = torch.empty(rec.shape, dtype=torch.float64, pin_memory=True)
         self._status_host.copy_(rec, non_blocking=True)
@@ -442,6 +445,7 @@ class Reconstruction:
         if getattr(self, "_status_host", None) is None:
             self._queue_status()
         self._status_event.synchronize()
+        self._status_checked = True
         rec = self._status_host.numpy().reshape(self.depth, 6)
         self.solve_stats = {d: dict(iters=int(rec[d, 0]), status=int(rec[d, 1]), replacements=int(rec[d, 2]),
                                     resid=float(rec[d, 4]), bnorm=float(rec[d, 5])) for d in range(self.depth)}
@@ -517,6 +521,10 @@ class Reconstruction:
                 pc = torch.empty(1, dtype=torch.int64, device=dev)
                 ws = L.grid_finalize(pg, pw, pc)
                 npar = int(pc.item())
+                if not self._status_checked:
+                    # first synchronisation after the solves: their status copy has landed; a failed
+                    # solve raises here, before any mesh is built from its result
+                    self.check_solves()
                 parents = torch.empty((npar, 3), dtype=torch.int32, device=dev)
                 L.call("ngs_grid_emit_coords", pg, L.ptr(parents), st)
                 cells = torch.empty((npar * 8, 3), dtype=torch.int32, device=dev)
@@ -612,6 +620,21 @@ class Reconstruction:
         # field at the primal samples
         vals = (self.chi_cells(pos) if n_upsample == 2 else self.chi_raw(pos)) - mean
         self._mark("chi")
+        verts, faces = self.marching_cubes(acc, cnt, pos, vals, total)
+        self._mark("mesh")
+        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_ids=acc, cnt=cnt, values=vals,
+                              positions=pos, counts=counts, starts=starts)
+        return verts, faces
+
+    def marching_cubes(self, acc, cnt, pos, vals, n_primal=None):
+        """Dual marching cubes over the complete dual cubes (count 8) and vertex de-duplication by
+        corner-id pair (dual_mc.cu:33-189, reconstructor.py:379-383): vertices [V, 3], faces [F, 3].
+        ``vals`` are the field values at the primal samples ``pos`` (any source: the mesh of a field
+        computed elsewhere goes through the same kernels)."""
+        st, dev = L.stream(), self.dev
+        nd = cnt.shape[0]
+        total = pos.shape[0] if n_primal is None else n_primal
+        vals = vals.contiguous().float()
         # marching cubes
         vcount = torch.empty(nd, dtype=torch.int32, device=dev)
         L.call("ngs_dual_mc_count", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(vals), L.ptr(vcount), st)
@@ -636,9 +659,7 @@ class Reconstruction:
         verts = torch.empty((nvert, 3), dtype=torch.float32, device=dev)
         L.call("ngs_vdedup_emit", L.ptr(vids), L.ptr(tris), nv, L.ptr(bstart), L.ptr(fill), L.ptr(sorted_keys),
                L.ptr(vid_of), L.ptr(faces), L.ptr(verts), st)
-        self._mark("mesh")
-        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_ids=acc, cnt=cnt, values=vals,
-                              positions=pos, counts=counts, starts=starts)
+        self.mesh_vids = vids          # (larger, smaller) primal-sample pair of every triangle corner
         return verts, faces.view(-1, 3)
 
     def dual_cubes(self) -> torch.Tensor:
@@ -677,5 +698,6 @@ class Reconstruction:
     def run(self, n_upsample: int = 2):
         self.build_tree().assemble().solve()
         mesh = self.extract_mesh(n_upsample)
-        self.check_solves()            # the mesh extraction has synchronised: no extra wait
+        if not self._status_checked:
+            self.check_solves()        # the mesh extraction has synchronised: no extra wait
         return mesh
