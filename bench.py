@@ -185,40 +185,51 @@ def run_reference(args, rank):
 
 # ----------------------------------------------------------------------------- learned-basis leg
 def learned_leg(n_shapes=32):
-    """Neural Galerkin forward + adjoint on ``n_shapes`` random superquadrics (3,000 points, voxel
-    1/128, 3 levels, AdditiveHermite basis with 18 features per voxel ~ init + N(0, 0.1), loss = MSE of
-    chi at 20,000 queries against the analytic target): device time per shape."""
+    """Neural Galerkin forward + adjoint on a batch of ``n_shapes`` random superquadrics (3,000
+    points, voxel 1/128, 3 levels, AdditiveHermite basis with 18 features per voxel ~ init + N(0,
+    0.1), loss = MSE of chi at 20,000 queries against the analytic target): the whole batch goes
+    through one Galerkin solve function (every level's solves of all shapes in one batched launch,
+    forward and adjoint); device time of the batch."""
     import torch
     from jspsr import synthetic
-    from jspsr.core.learned import LearnedStep
-    fw, bw, loss = [], [], []
-    voxels = []
-    for seed in range(n_shapes + 1):
-        xyz, nrm, q, tgt = synthetic.learned_problem(seed=seed)
-        T = lambda a: torch.from_numpy(a).cuda()     # noqa: E731
-        s = LearnedStep(T(xyz), T(nrm), T(q), T(tgt), min_density=None).build()
-        feats = s.init_features(0.1, seed=seed)
-        n = s.normal.clone().requires_grad_(True)
-        f = {d: v.clone().requires_grad_(True) for d, v in feats.items()}
+    from jspsr.core.learned import LearnedBatch, LearnedStep
+
+    def make(seeds):
+        steps = []
+        for seed in seeds:
+            xyz, nrm, q, tgt = synthetic.learned_problem(seed=seed)
+            T = lambda a: torch.from_numpy(a).cuda()     # noqa: E731
+            steps.append(LearnedStep(T(xyz), T(nrm), T(q), T(tgt), min_density=None).build())
+        return LearnedBatch(steps)
+
+    def run(batch):
+        feats = [st.init_features(0.1, seed=k) for k, st in enumerate(batch.steps)]
+        normals = [st.normal.clone().requires_grad_(True) for st in batch.steps]
+        fl = [{d: v.clone().requires_grad_(True) for d, v in f.items()} for f in feats]
         torch.cuda.synchronize()
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         e[0].record()
-        lo, _, _ = s.forward(n, f)
+        total, losses, _ = batch.forward(normals, fl)
         e[1].record()
-        lo.backward()
+        total.backward()
         e[2].record()
         torch.cuda.synchronize()
-        if seed == 0:
-            continue                     # first shape: warm-up (table upload, allocator)
-        fw.append(e[0].elapsed_time(e[1]))
-        bw.append(e[1].elapsed_time(e[2]))
-        loss.append(float(lo.detach()))
-        voxels.append(sum(s.tree.get_coords_size(s.tree.DECODER, d) for d in range(s.depth)))
-    return {"shapes": n_shapes, "forward_ms_per_shape": float(np.mean(fw)), "adjoint_ms_per_shape": float(np.mean(bw)),
-            "shapes_per_s": 1e3 / float(np.mean(np.add(fw, bw))), "mean_voxels": float(np.mean(voxels)),
+        return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), [float(x) for x in losses]
+
+    warm = make(range(1000, 1002))
+    run(warm)                                    # table uploads, allocator, kernels
+    batch = make(range(n_shapes))
+    batch.geometry()                             # positions only: built once per shape set
+    fw, bw, losses = run(batch)
+    voxels = [sum(st.tree.get_coords_size(st.tree.DECODER, d) for d in range(st.depth)) for st in batch.steps]
+    return {"shapes": n_shapes, "batch_forward_ms": fw, "batch_adjoint_ms": bw,
+            "forward_ms_per_shape": fw / n_shapes, "adjoint_ms_per_shape": bw / n_shapes,
+            "shapes_per_s": 1e3 * n_shapes / (fw + bw), "mean_voxels": float(np.mean(voxels)),
+            "mean_loss": float(np.mean(losses)),
             "config": "3,000 points + N(0,0.005) on a random superquadric, voxel 1/128, 3 levels, "
-                      "AdditiveHermite(6, SinPeaks(1..3)) 18 features/voxel, 20,000 queries, cholmod-equivalent "
-                      "FP64-refined solves forward and adjoint; gradients w.r.t. normals and features"}
+                      "AdditiveHermite(6, SinPeaks(1..3)) 18 features/voxel, 20,000 queries, FP64 PCG to 1e-12 "
+                      "forward and adjoint (cholmod-equivalent); gradients w.r.t. normals and features; "
+                      "32 shapes in one batched Galerkin solve"}
 
 
 # ----------------------------------------------------------------------------- serving leg
@@ -296,8 +307,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-comparators", action="store_true")
     ap.add_argument("--workload", default="superquadrics-300k", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="all", choices=["all", "recon", "learned", "serving"],
-                    help="all: reconstruction line with the learned-basis and serving legs attached")
+    ap.add_argument("--mode", default="all", choices=["all", "recon", "learned", "serving", "profile"],
+                    help="all: reconstruction line with the learned-basis and serving legs attached; profile: "
+                         "warm-up reconstructions, then one between cudaProfilerStart/Stop (for ncu "
+                         "--profile-from-start off)")
     ap.add_argument("--serving-requests", type=int, default=1024)
     ap.add_argument("--learned-shapes", type=int, default=32)
     ap.add_argument("--serving-slots", type=int, default=8)
@@ -345,6 +358,16 @@ def main():
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    if args.mode == "profile":
+        torch.cuda.profiler.start()
+        step()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        if rank == 0:
+            print(json.dumps({"mode": "profile", "workload": W["workload"], "profiled_steps": 1}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     def barrier():
         if world > 1:

@@ -128,6 +128,27 @@ int ngs_grid_neighbours_fill(ngs_grid g, const int64_t* row_of_rank, const void*
                              const uint32_t* masks, const int64_t* start, int64_t* src_ids, int64_t* tgt_ids,
                              int32_t* kidx, ngs_stream s);
 
+/* ======================================================================= nearest neighbours, signed distance
+ * Exact k-nearest-neighbour search on a uniform cell grid and the signed distance from oriented
+ * points (ref: ext/sdfgen/sdf_from_points.cu:31-116 with the k-d tree of
+ * csrc/common/kdtree_cuda.cu:1071-1279; Python binding ext/__init__.py:11-16).  g: a zeroed grid of
+ * stride 1 in cell units (cell side h = 1 / inv_h) over the reference points' cells.
+ * mark_cells marks the occupied cells (then ngs_grid_finalize); bucket writes every point's cell row
+ * (cell_of) and the counts per cell (cell_count, zeroed); the caller scans the counts into start
+ * (int64 [cells + 1]); scatter fills sorted (int32 [n], the points cell by cell; cursor int32
+ * [cells], zeroed).  knn_sdf: per query the k <= 32 nearest points (idx_out int32 [q, k], d2_out
+ * float [q, k] squared distances, nearest first, ties to the smaller index; either may be NULL) and,
+ * when sdf_out is given, the signed distance with the reference's rule (magnitude from the nearest
+ * point, |n.(q-p)| within stdv, |q-p| beyond; negative unless more than k/2 normals face the query). */
+int ngs_knn_mark_cells(ngs_grid g, const float* xyz, int64_t n, float inv_h, ngs_stream s);
+int ngs_knn_bucket(ngs_grid g, const float* xyz, int64_t n, float inv_h, int32_t* cell_of, int32_t* cell_count,
+                   ngs_stream s);
+int ngs_knn_scatter(const int32_t* cell_of, int64_t n, const int64_t* start, int32_t* cursor, int32_t* sorted,
+                    ngs_stream s);
+int ngs_knn_sdf(ngs_grid g, const int64_t* start, const int32_t* sorted, const float* ref_xyz, const float* ref_normal,
+                const float* queries, int64_t nq, float inv_h, float h, int k, float stdv, int32_t* idx_out,
+                float* d2_out, float* sdf_out, ngs_stream s);
+
 /* min/max of a float [n,3] array -> bbox_dev float[6] = (min xyz, max xyz) */
 int ngs_points_bbox(const float* xyz, int64_t n, float* bbox_dev, ngs_stream s);
 /* Mark the 8 trilinear corner cells of every point with level <= max_level
@@ -270,6 +291,8 @@ typedef struct ngs_pcg_system {
   const float* inv_diag;     /* [n] */
   float* x32;                /* [n] out (REFERENCE, MIXED: FP32 copy of x) */
   double* x64;               /* [n] out (MIXED, FP64) */
+  const int16_t* col_delta;  /* [nnz] optional: column - row of every entry; when given the solver
+                                reads these 2-byte deltas instead of the 4-byte columns (NULL: cols) */
 } ngs_pcg_system;
 
 typedef struct ngs_pcg_config {
@@ -282,6 +305,10 @@ typedef struct ngs_pcg_config {
   double timeout_s;          /* bound of every device-side wait */
 } ngs_pcg_config;
 
+/* col_delta[j] = cols[j] - row(j) for a CSR whose every |column - row| fits int16 (the caller
+ * checks the bound; ref: no counterpart, the reference's SpMV reads int32 columns,
+ * csrc/sparse_solve/solve_pcg.cu:67-73). */
+int ngs_csr_col_delta(const int64_t* rowptr, const int32_t* cols, int64_t n, int16_t* col_delta, ngs_stream s);
 size_t ngs_pcg_workspace_bytes(int64_t n, int mode);
 /* info_dev: int64[4] = {iterations, status, replacements, reserved};
  * resid_dev: double[2] = {final |r|, |b|}.  Iterations and status are also valid

@@ -55,6 +55,7 @@ struct PcgArgs {
   int64_t nnz;
   const int64_t* rowptr;
   const int32_t* cols;
+  const int16_t* cols16;     // column - row per entry (2 bytes instead of 4), or NULL
   const void* vals;          // recurrence matrix (float or double)
   const double* vals64;      // replacement matrix (MIXED)
   const void* b;             // float (REFERENCE) or double
@@ -134,7 +135,7 @@ NGS_DEV T ld_mat(const T* p) {
 // row's product (lane 0 of its group) and returns a contribution to the thread's partial sum.
 // The gathered vector is read with plain loads: it was written earlier in this launch.  Ends with a
 // block barrier, after which every thread may read the rows written by the epilogue.
-template <bool STREAM, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
+template <bool STREAM, bool DELTA, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
 NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
                          Pre pre, Epi epi, double& dsum) {
   constexpr int L = PCG_ROW_LANES;
@@ -156,7 +157,8 @@ NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT
 #pragma unroll
       for (int k = 0; k < U; k++) {
         const int64_t j = j0 + (int64_t)k * L;
-        c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : (int32_t)row;
+        if constexpr (DELTA) c[k] = (int32_t)row + (j < e1 ? (int32_t)ld_mat<STREAM>(a.cols16 + j) : 0);
+        else c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : (int32_t)row;
         m[k] = j < e1 ? ld_mat<STREAM>(vals + j) : (MT)0;
       }
       VT xv[U];
@@ -185,8 +187,14 @@ NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT
 template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
 NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
                        Pre pre, Epi epi, double& dsum) {
-  if (a.evict_first) spmv_rows_t<true, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
-  else spmv_rows_t<false, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+  // the column encoding too: 2-byte deltas when the caller supplied them, 4-byte columns otherwise
+  if (a.cols16) {
+    if (a.evict_first) spmv_rows_t<true, true, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+    else spmv_rows_t<false, true, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+  } else {
+    if (a.evict_first) spmv_rows_t<true, false, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+    else spmv_rows_t<false, false, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+  }
 }
 
 // Grid synchronisation of a cooperative launch through one arrival counter in global memory (zeroed
@@ -725,8 +733,8 @@ static void pcg_clear_status(int64_t* info_dev, double* resid_dev, cudaStream_t 
 // Returns NGS_OK, an error, or 1 for an empty system (nothing to launch).  Touches no device memory.
 static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
                        int64_t* info_dev, double* resid_dev, cudaStream_t st, PcgArgs& a) {
-  if (!sys || !cfg || !info_dev || !resid_dev || sys->n < 0 || !sys->rowptr || (sys->nnz > 0 && !sys->cols) ||
-      !sys->inv_diag)
+  if (!sys || !cfg || !info_dev || !resid_dev || sys->n < 0 || !sys->rowptr ||
+      (sys->nnz > 0 && !sys->cols && !sys->col_delta) || !sys->inv_diag)
     return NGS_ERR_INVALID_ARG;
   const int mode = cfg->mode;
   if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64) return NGS_ERR_INVALID_ARG;
@@ -744,6 +752,7 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.nnz = sys->nnz;
   a.rowptr = sys->rowptr;
   a.cols = sys->cols;
+  a.cols16 = sys->col_delta;
   a.vals = mode == NGS_PCG_FP64 ? (const void*)sys->vals64 : (const void*)sys->vals32;
   a.vals64 = sys->vals64;
   a.b = mode == NGS_PCG_REFERENCE ? (const void*)sys->b32 : (const void*)sys->b64;
@@ -769,7 +778,7 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.wait_ns = (unsigned long long)(timeout * 1e9);
   a.budget_ns = a.wait_ns;
   a.inner_rtol = 1.0e-4;
-  const size_t mat_bytes = (size_t)sys->nnz * (4 + (mode == NGS_PCG_FP64 ? 8 : 4));
+  const size_t mat_bytes = (size_t)sys->nnz * ((sys->col_delta ? 2 : 4) + (mode == NGS_PCG_FP64 ? 8 : 4));
   a.evict_first = mat_bytes > (size_t)96 << 20;
   return NGS_OK;
 }
@@ -913,6 +922,24 @@ extern "C" int ngs_pcg_solve_noalloc(const ngs_pcg_system* sys, const ngs_pcg_co
   // and the kernel initialises every vector and writes each partial before reading it, so what the
   // previous call left in the shared scratch does not matter.
   return ngs_pcg_solve(sys, cfg, ws, kNoallocScratchBytes, info_dev, resid_dev, s);
+}
+
+// ----------------------------------------------------------------------------- 2-byte column deltas
+__global__ void col_delta_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ cols, int64_t n,
+                                 int16_t* __restrict__ out) {
+  const int sub = threadIdx.x & 7;
+  const int64_t groups = (int64_t)gridDim.x * (blockDim.x / 8);
+  for (int64_t row = ngs_gtid() / 8; row < n; row += groups)
+    for (int64_t j = rp[row] + sub; j < rp[row + 1]; j += 8) out[j] = (int16_t)(cols[j] - (int32_t)row);
+}
+
+extern "C" int ngs_csr_col_delta(const int64_t* rowptr, const int32_t* cols, int64_t n, int16_t* col_delta,
+                                 ngs_stream s) {
+  if (n < 0 || (n > 0 && (!rowptr || !cols || !col_delta))) return NGS_ERR_INVALID_ARG;
+  if (n == 0) return NGS_OK;
+  { ngs_count_launch(); col_delta_kernel<<<ngs_blocks(n * 8, 256), 256, 0, (cudaStream_t)s>>>(rowptr, cols, n, col_delta); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
 }
 
 // ----------------------------------------------------------------------------- FP64 building blocks

@@ -38,7 +38,8 @@ class HashTable(C.Structure):
 
 class PcgSystem(C.Structure):
     _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("rowptr", vp), ("cols", vp), ("vals32", vp),
-                ("vals64", vp), ("b32", vp), ("b64", vp), ("inv_diag", vp), ("x32", vp), ("x64", vp)]
+                ("vals64", vp), ("b32", vp), ("b64", vp), ("inv_diag", vp), ("x32", vp), ("x64", vp),
+                ("col_delta", vp)]
 
 
 class PcgConfig(C.Structure):
@@ -82,6 +83,10 @@ _SIGS = {
                                    vp, vp], C.c_int),
     "ngs_grid_neighbours_fill": ([G, vp, vp, C.c_int, i64, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, vp,
                                   vp, vp], C.c_int),
+    "ngs_knn_mark_cells": ([G, vp, i64, f32, vp], C.c_int),
+    "ngs_knn_bucket": ([G, vp, i64, f32, vp, vp, vp], C.c_int),
+    "ngs_knn_scatter": ([vp, i64, vp, vp, vp, vp], C.c_int),
+    "ngs_knn_sdf": ([G, vp, vp, vp, vp, vp, i64, f32, f32, C.c_int, f32, vp, vp, vp, vp], C.c_int),
     "ngs_splat_weights": ([G, vp, i64, f32, f64, vp, vp], C.c_int),
     "ngs_density_eval": ([G, vp, i64, f32, f64, vp, f32, C.c_int, vp, vp, vp, vp], C.c_int),
     "ngs_splat_data": ([G, vp, i64, f32, f64, vp, C.c_int, vp, vp, C.c_int, f32, vp, vp], C.c_int),
@@ -102,6 +107,7 @@ _SIGS = {
     "ngs_correction_stiffness": ([vp, i64, C.c_int, G, vp, vp, vp, C.c_int, vp, vp], C.c_int),
     "ngs_correction_screen": ([vp, vp, i64, vp, vp, f64, vp, vp], C.c_int),
     "ngs_finish_system": ([vp, i64, vp, i64, vp, vp, vp], C.c_int),
+    "ngs_csr_col_delta": ([vp, vp, i64, vp, vp], C.c_int),
     "ngs_pcg_workspace_bytes": ([i64, C.c_int], sz),
     "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
     "ngs_pcg_block_capacity": ([C.c_int], C.c_int),

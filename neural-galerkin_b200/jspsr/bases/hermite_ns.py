@@ -21,7 +21,9 @@ def _get_ns(n_degrees):
 
 class AdditiveHermite(AdditiveBasis):
     def __init__(self, n_degrees, components, init_vals):
-        assert n_degrees > 3, "Degrees <= cubic does not admit two hermite constraints!"
+        if n_degrees <= 3:
+            raise ValueError(f"a polynomial part of degree {n_degrees} leaves no freedom once value and slope "
+                             "vanish at both ends; use degree 4 or more")
         comps = list(components)
         super().__init__(comps + [Power(p) for p in range(n_degrees + 1)],
                          list(init_vals) + [0.0] * (n_degrees + 1))

@@ -4,7 +4,9 @@ The flow of the reference's training step (``models/full_net.py:118-133`` with t
 ``jspsr/__init__.py:36-47``): density-adaptive tree, normals splatted with 1/density weights,
 ``Reconstructor.solve_multigrid`` with an ``AdditiveHermite`` basis and per-voxel features, field
 evaluated at query points, MSE loss against a target field, gradients w.r.t. the normals and the
-per-voxel basis features through the autograd graph of assembly, screening and the linear solves.
+per-voxel basis features.  Assembly and solve are one ``galerkin.GalerkinSolve`` with a hand-written
+adjoint; ``LearnedBatch`` runs many shapes through one such function, so that every level's forward
+and adjoint solves of all shapes go to the device as one batched persistent PCG launch.
 """
 from __future__ import annotations
 
@@ -16,6 +18,7 @@ import torch
 
 from ..bases.hermite_ns import AdditiveHermite
 from ..bases.additive_components import SinPeaks
+from . import galerkin as G
 from ._hash_backend import compute_density
 from .hashtree import HashTree
 from .reconstructor import Reconstructor
@@ -91,3 +94,38 @@ class LearnedStep:
         loss, chi, rec = self.forward(n, f)
         loss.backward()
         return float(loss.detach()), n.grad, {d: v.grad for d, v in f.items()}, chi.detach(), rec
+
+
+class LearnedBatch:
+    """Many shapes of the learned form at once: one ``GalerkinSolve`` for all of them."""
+
+    def __init__(self, steps):
+        self.steps = [st if st.tree is not None else st.build() for st in steps]
+        self.basis = self.steps[0].basis
+        self.shapes = None
+
+    def geometry(self):
+        """Geometry of every shape (depends on the positions only; built once)."""
+        if self.shapes is None:
+            self.shapes = []
+            for st in self.steps:
+                data_levels = [d for d in range(st.depth) if bool(torch.any(st.tree.xyz_depth == d))]
+                self.shapes.append(G.ShapeGeometry.build(st.tree, st.tree.DECODER, st.depth - 1, 0, data_levels,
+                                                         st.xyz, st.screen_alpha, 0.1,
+                                                         self.basis.get_domain_range()))
+        return self.shapes
+
+    def forward(self, normals, feats_list):
+        """(summed loss, per-shape losses, per-shape chi at the queries); differentiable in every
+        shape's normals and features."""
+        shapes = self.geometry()
+        nd_list = [st.normal_data(n) for st, n in zip(self.steps, normals)]
+        sols = G.galerkin_solve(self.basis, shapes, feats_list, nd_list, self.steps[0].solver)
+        losses, chis = [], []
+        for st, f, x in zip(self.steps, feats_list, sols):
+            chi_pts = sum(st.tree.evaluate_interpolated(st.xyz, self.basis, f[d], d, x[d]) for d in x)
+            iso = (chi_pts * st.sample_weight).sum() / st.sample_weight.sum()
+            chi = sum(st.tree.evaluate_interpolated(st.query, self.basis, f[d], d, x[d]) for d in x) - iso
+            losses.append(torch.mean((chi - st.target) ** 2))
+            chis.append(chi)
+        return torch.stack(losses).sum(), losses, chis

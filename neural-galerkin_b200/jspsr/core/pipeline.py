@@ -107,6 +107,8 @@ class Level:
     x32: torch.Tensor = None
     info: torch.Tensor = None
     resid: torch.Tensor = None
+    col_delta: torch.Tensor = None   # int16 column - row per non-zero (when every delta fits)
+    delta_ok: bool = False
 
 
 def _box(qmin, qmax, stride, pad=1):
@@ -135,7 +137,173 @@ class Timings:
         return out
 
 
-class Reconstruction:
+class DualMesher:
+    """The mesh stage shared by the device pipeline and the reference-API ``Reconstructor``: needs
+    ``levels`` (objects with a ``stride``), ``vs``, ``dev`` and ``dual_grid_max_words``."""
+    dual_grid_max_words = 1 << 27
+    t = None
+
+    def _mark(self, name):
+        if self.t is not None:
+            self.t.mark(name)
+
+    def mesh_from_leaves(self, base: dict, max_depth: int, n_upsample: int, field):
+        """Dual marching cubes over the conformal leaf cells ``base[d]`` (int32 [M_d, 3] per level):
+        each cell expanded into n_upsample^3 samples, dual centres = the samples' unique corners, the 8
+        primal samples of every dual cube accumulated through the dual grid, the field evaluated at
+        the samples by ``field(positions)`` (values relative to the iso level), then the cubes'
+        triangles and the vertex de-duplication (reconstructor.py:338-397)."""
+        st = L.stream()
+        dev = self.dev
+        # expanded primal cells and their sample positions
+        evs = np.float32(self.vs / n_upsample)
+        e3 = n_upsample ** 3
+        counts = [base[d].shape[0] * e3 for d in range(max_depth)]
+        total = sum(counts)
+        epb = torch.empty((total, 3), dtype=torch.int32, device=dev)
+        pos = torch.empty((total, 3), dtype=torch.float32, device=dev)
+        starts = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        for d in range(max_depth):
+            L.call("ngs_expand_cells", L.ptr(base[d]), base[d].shape[0], n_upsample, self.levels[d].stride, evs,
+                   L.ptr(epb[starts[d]:]), L.ptr(pos[starts[d]:]), st)
+        # dual centres: unique corners of all expanded cells
+        # box of the corners actually present (the cells' extent, not the levels' padded boxes: with
+        # many levels the coarse boxes would make the bitmap far larger than the surface needs)
+        ext = []
+        for d in range(max_depth):
+            if counts[d] == 0:
+                continue
+            # the expanded cells of level d span base * n_up .. base * n_up + (n_up - 1) * stride, and
+            # their corners one stride further: the extent follows from the (n_up^3 times fewer) cells
+            c = base[d]
+            s = self.levels[d].stride
+            ext.append(torch.cat([c.min(0).values.long() * n_upsample, c.max(0).values.long() * n_upsample + n_upsample * s]))
+        ext = torch.stack(ext).cpu().numpy()
+        lo = ext[:, :3].min(0)
+        hi = ext[:, 3:].max(0)
+        dims = (hi - lo) + 1
+        offs = L.device_table("conform_offsets", lambda: CONFORM_OFFSETS, dev)
+        box_words = int(dims[0]) * int(dims[1]) * ((int(dims[2]) + 63) // 64)
+        if box_words <= self.dual_grid_max_words:
+            # rank bitmap over the box: dual centres ranked without a sort
+            dg, dw = L.make_grid(lo, dims, 1, dev)
+            for d in range(max_depth):
+                if n_upsample == 2:
+                    L.call("ngs_grid_mark_cell_corners", dg, L.ptr(base[d]), base[d].shape[0], self.levels[d].stride, st)
+                else:
+                    L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
+                           self.levels[d].stride, st)
+            dcount = torch.empty(1, dtype=torch.int64, device=dev)
+            self._dual_ws = L.grid_finalize(dg, dw, dcount)
+            nd = int(dcount.item())
+            acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
+            cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
+            for d in range(max_depth):
+                if n_upsample == 2 and self.levels[d].stride == 1:
+                    L.call("ngs_dual_mc_indices_cells", dg, L.ptr(base[d]), base[d].shape[0], d, int(starts[d]),
+                           L.ptr(acc), 1, L.ptr(cnt), st)
+                else:
+                    L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride,
+                           d, int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
+        else:
+            # deep hierarchies: the coarse cells stretch the box far beyond the surface, so the
+            # dual centres are de-duplicated by a sort of packed corner keys and found through the
+            # key table instead (the reference's own route, reconstructor.py:347-357)
+            if np.any(dims >= (1 << 21)):
+                raise ValueError(f"mesh domain of {dims.tolist()} cells exceeds 2^21 cells per axis")
+            nd, table = self._dual_centres_by_sort(epb, starts, counts, max_depth, lo, offs)
+            acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
+            cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
+            for d in range(max_depth):
+                L.call("ngs_dual_mc_indices_hash", L.C.byref(table.table), L.ptr(epb[starts[d]:]), counts[d],
+                       self.levels[d].stride, d, int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
+            self._dual_ws = table
+        # the cubes with all 8 corners (cnt == 8) are the reference's compacted list; nearly every
+        # centre is one, so the count and emit passes skip the others in place instead of
+        # compacting acc first (same triangles, same order); dual_cubes() compacts on request
+        self.topology_overflow = cnt  # counts above 8 mark the reference's "Topology Error"
+        self._mark("dual grid")
+        # field at the primal samples
+        vals = field(pos)
+        self._mark("chi")
+        verts, faces = self.marching_cubes(acc, cnt, pos, vals, total)
+        self._mark("mesh")
+        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_ids=acc, cnt=cnt, values=vals,
+                              positions=pos, counts=counts, starts=starts)
+        return verts, faces
+
+    def marching_cubes(self, acc, cnt, pos, vals, n_primal=None):
+        """Dual marching cubes over the complete dual cubes (count 8) and vertex de-duplication by
+        corner-id pair (dual_mc.cu:33-189, reconstructor.py:379-383): vertices [V, 3], faces [F, 3].
+        ``vals`` are the field values at the primal samples ``pos`` (any source: the mesh of a field
+        computed elsewhere goes through the same kernels)."""
+        st, dev = L.stream(), self.dev
+        nd = cnt.shape[0]
+        total = pos.shape[0] if n_primal is None else n_primal
+        vals = vals.contiguous().float()
+        # marching cubes
+        vcount = torch.empty(nd, dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_count", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(vals), L.ptr(vcount), st)
+        voff, vtot = L.scan(vcount)
+        nv = int(vtot.item())
+        tris = torch.empty((nv, 3), dtype=torch.float32, device=dev)
+        vids = torch.empty((nv, 2), dtype=torch.int32, device=dev)
+        L.call("ngs_dual_mc_emit", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris),
+               L.ptr(vids), st)
+        # vertex de-duplication by (vid0, vid1) (reconstructor.py:380-383)
+        bcount = torch.zeros(total, dtype=torch.int32, device=dev)
+        L.call("ngs_vdedup_count", L.ptr(vids), nv, L.ptr(bcount), st)
+        bstart, _ = L.scan(bcount)
+        fill = torch.zeros(total, dtype=torch.int32, device=dev)
+        sorted_keys = torch.empty(nv, dtype=torch.int64, device=dev)
+        first = torch.empty(nv, dtype=torch.int32, device=dev)
+        L.call("ngs_vdedup_sort", L.ptr(vids), nv, L.ptr(bstart), total, L.ptr(fill), L.ptr(sorted_keys),
+               L.ptr(first), st)
+        vid_of, nvert_t = L.scan(first)
+        nvert = int(nvert_t.item())
+        faces = torch.empty(nv, dtype=torch.int64, device=dev)
+        verts = torch.empty((nvert, 3), dtype=torch.float32, device=dev)
+        L.call("ngs_vdedup_emit", L.ptr(vids), L.ptr(tris), nv, L.ptr(bstart), L.ptr(fill), L.ptr(sorted_keys),
+               L.ptr(vid_of), L.ptr(faces), L.ptr(verts), st)
+        self.mesh_vids = vids          # (larger, smaller) primal-sample pair of every triangle corner
+        return verts, faces.view(-1, 3)
+
+    def dual_cubes(self) -> torch.Tensor:
+        """The complete dual cubes of the last extract_mesh (count 8), in dual-centre order: the
+        reference's compacted [M, 8, 2] (primal id, depth) list (reconstructor.py:366)."""
+        acc, cnt = self.mesh_info["acc_ids"], self.mesh_info["cnt"]
+        nd = cnt.shape[0]
+        st = L.stream()
+        keep = torch.empty(nd, dtype=torch.int32, device=self.dev)
+        L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
+        koff, ktot = L.scan(keep)
+        m = int(ktot.item())
+        ids = torch.empty((m, 8), dtype=torch.int32, device=self.dev)
+        L.call("ngs_dual_mc_compact", L.ptr(acc), 1, L.ptr(keep), L.ptr(koff), nd, L.ptr(ids), st)
+        # the depth of a primal sample is the level whose segment holds its id
+        bounds = torch.as_tensor(np.asarray(self.mesh_info["starts"][1:], dtype=np.int64), device=self.dev)
+        depth = torch.bucketize(ids.long(), bounds, right=True).int()
+        return torch.stack([ids, depth], dim=2)
+
+    def _dual_centres_by_sort(self, epb, starts, counts, max_depth, lo, offs):
+        """Unique corners of the expanded cells, in lexicographic order, and a key table over them."""
+        from ..ext import HashLookupData, hash_cuda
+        lo_t = torch.as_tensor(lo, dtype=torch.int64, device=self.dev)
+        keys = []
+        for d in range(max_depth):
+            c = epb[starts[d]:starts[d] + counts[d]]
+            if c.shape[0] == 0:
+                continue
+            corners = (c[:, None, :].long() + offs.long()[None] * self.levels[d].stride).reshape(-1, 3) - lo_t
+            keys.append((corners[:, 0] << 42) | (corners[:, 1] << 21) | corners[:, 2])
+        uk = torch.unique(torch.cat(keys))           # sorted: packed keys order like (x, y, z)
+        mask = (1 << 21) - 1
+        dual = (torch.stack([uk >> 42, (uk >> 21) & mask, uk & mask], 1) + lo_t).int()
+        return int(uk.numel()), HashLookupData(hash_cuda(dual), None, False)
+
+
+
+class Reconstruction(DualMesher):
     """One reconstruction, every buffer device-resident."""
 
     def __init__(self, xyz: torch.Tensor, normal: torch.Tensor, voxel_size: float, depth: int = 4,
@@ -251,9 +419,14 @@ class Reconstruction:
             lv.rowptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
             L.scan(counts, out=lv.rowptr[:lv.n], total=lv.rowptr[lv.n:])
         self._mark("structure")
-        nnz = torch.stack([lv.rowptr[lv.n] for lv in self.levels]).cpu().numpy()
+        # with the non-zero counts, a bound on |column - row| per level: a voxel's stencil spans the x
+        # slabs x-2 .. x+2, whose rows lie between the first rank of slab x-2 and the last of slab x+2
+        span = [self._row_span_bound(lv) for lv in self.levels]
+        host = torch.stack([lv.rowptr[lv.n] for lv in self.levels] + span).cpu().numpy()
+        nnz, span = host[:self.depth], host[self.depth:]
         for d, lv in enumerate(self.levels):
             lv.nnz = int(nnz[d])
+            lv.delta_ok = bool(span[d] <= 32767)
             lv.cols = torch.empty(lv.nnz, dtype=torch.int32, device=self.dev)
             lv.vals64 = torch.empty(lv.nnz, dtype=torch.float64, device=self.dev)
             lv.diag_slot = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
@@ -269,12 +442,27 @@ class Reconstruction:
                 lv.group = (keys, order)          # reused by the screening RHS terms of this level
                 L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(order),
                        L.ptr(keys), L.ptr(lv.masks), L.ptr(lv.rowptr), sf * self.alpha, L.ptr(lv.vals64), st)
+            if lv.delta_ok:
+                # 2-byte column deltas for the solver's SpMV (6 instead of 8 bytes per non-zero)
+                lv.col_delta = torch.empty(lv.nnz, dtype=torch.int16, device=self.dev)
+                L.call("ngs_csr_col_delta", L.ptr(lv.rowptr), L.ptr(lv.cols), lv.n, L.ptr(lv.col_delta), st)
             lv.vals32 = torch.empty(lv.nnz, dtype=torch.float32, device=self.dev)
             lv.inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
             L.call("ngs_finish_system", L.ptr(lv.vals64), lv.nnz, L.ptr(lv.diag_slot), lv.n, L.ptr(lv.vals32),
                    L.ptr(lv.inv_diag), st)
         self._mark("assembly")
         return self
+
+    @staticmethod
+    def _row_span_bound(lv: Level) -> torch.Tensor:
+        """Device scalar >= max |column - row| of the level's 5^3-stencil matrix: rows are ranks in
+        (x, y, z) order, so the rows of the stencil of a voxel in x slab i lie in slabs i-2 .. i+2."""
+        g = lv.grid
+        d0, per_slab = int(g.dims[0]), int(g.dims[1]) * int(g.zwords)
+        first = lv.words.view(torch.int32).view(-1, 4)[::per_slab, 0][:d0].long()
+        starts = torch.cat([first, torch.full((1,), lv.n, dtype=torch.int64, device=first.device)])
+        i = torch.arange(d0, device=first.device)
+        return (starts[(i + 3).clamp(max=d0)] - starts[(i - 2).clamp(min=0)]).max()
 
     # ------------------------------------------------------------------ RHS + solve
     def _rhs(self, d):
@@ -331,6 +519,7 @@ class Reconstruction:
         b32 = lv.rhs.float()
         sysd.b32, sysd.b64 = b32.data_ptr(), lv.rhs.data_ptr()
         sysd.x32, sysd.x64 = lv.x32.data_ptr(), lv.x64.data_ptr()
+        sysd.col_delta = lv.col_delta.data_ptr() if lv.col_delta is not None else None
         cfg = item.cfg
         cfg.mode, cfg.max_iter, cfg.tol = spec.mode, spec.maxiter, spec.tol
         cfg.res_fix, cfg.replace_every, cfg.blocks, cfg.timeout_s = int(spec.res_fix), spec.replace, 0, spec.timeout
@@ -549,151 +738,8 @@ class Reconstruction:
             L.call("ngs_compact_coords", L.ptr(base[d]), L.ptr(leaf), L.ptr(off), base[d].shape[0], L.ptr(out), st)
             base[d] = out
         self._mark("leaves")
-        # expanded primal cells and their sample positions
-        evs = np.float32(self.vs / n_upsample)
-        e3 = n_upsample ** 3
-        counts = [base[d].shape[0] * e3 for d in range(max_depth)]
-        total = sum(counts)
-        epb = torch.empty((total, 3), dtype=torch.int32, device=dev)
-        pos = torch.empty((total, 3), dtype=torch.float32, device=dev)
-        starts = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-        for d in range(max_depth):
-            L.call("ngs_expand_cells", L.ptr(base[d]), base[d].shape[0], n_upsample, self.levels[d].stride, evs,
-                   L.ptr(epb[starts[d]:]), L.ptr(pos[starts[d]:]), st)
-        # dual centres: unique corners of all expanded cells
-        # box of the corners actually present (the cells' extent, not the levels' padded boxes: with
-        # many levels the coarse boxes would make the bitmap far larger than the surface needs)
-        ext = []
-        for d in range(max_depth):
-            if counts[d] == 0:
-                continue
-            # the expanded cells of level d span base * n_up .. base * n_up + (n_up - 1) * stride, and
-            # their corners one stride further: the extent follows from the (n_up^3 times fewer) cells
-            c = base[d]
-            s = self.levels[d].stride
-            ext.append(torch.cat([c.min(0).values.long() * n_upsample, c.max(0).values.long() * n_upsample + n_upsample * s]))
-        ext = torch.stack(ext).cpu().numpy()
-        lo = ext[:, :3].min(0)
-        hi = ext[:, 3:].max(0)
-        dims = (hi - lo) + 1
-        offs = L.device_table("conform_offsets", lambda: CONFORM_OFFSETS, dev)
-        box_words = int(dims[0]) * int(dims[1]) * ((int(dims[2]) + 63) // 64)
-        if box_words <= self.dual_grid_max_words:
-            # rank bitmap over the box: dual centres ranked without a sort
-            dg, dw = L.make_grid(lo, dims, 1, dev)
-            for d in range(max_depth):
-                if n_upsample == 2:
-                    L.call("ngs_grid_mark_cell_corners", dg, L.ptr(base[d]), base[d].shape[0], self.levels[d].stride, st)
-                else:
-                    L.call("ngs_grid_mark_coords", dg, L.ptr(epb[starts[d]:]), counts[d], L.ptr(offs), 8,
-                           self.levels[d].stride, st)
-            dcount = torch.empty(1, dtype=torch.int64, device=dev)
-            self._dual_ws = L.grid_finalize(dg, dw, dcount)
-            nd = int(dcount.item())
-            acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
-            cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
-            for d in range(max_depth):
-                if n_upsample == 2 and self.levels[d].stride == 1:
-                    L.call("ngs_dual_mc_indices_cells", dg, L.ptr(base[d]), base[d].shape[0], d, int(starts[d]),
-                           L.ptr(acc), 1, L.ptr(cnt), st)
-                else:
-                    L.call("ngs_dual_mc_indices_grid", dg, L.ptr(epb[starts[d]:]), counts[d], self.levels[d].stride,
-                           d, int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
-        else:
-            # deep hierarchies: the coarse cells stretch the box far beyond the surface, so the
-            # dual centres are de-duplicated by a sort of packed corner keys and found through the
-            # key table instead (the reference's own route, reconstructor.py:347-357)
-            if np.any(dims >= (1 << 21)):
-                raise ValueError(f"mesh domain of {dims.tolist()} cells exceeds 2^21 cells per axis")
-            nd, table = self._dual_centres_by_sort(epb, starts, counts, max_depth, lo, offs)
-            acc = torch.zeros((nd, 8), dtype=torch.int32, device=dev)
-            cnt = torch.zeros(nd, dtype=torch.int32, device=dev)
-            for d in range(max_depth):
-                L.call("ngs_dual_mc_indices_hash", L.C.byref(table.table), L.ptr(epb[starts[d]:]), counts[d],
-                       self.levels[d].stride, d, int(starts[d]), L.ptr(acc), 1, L.ptr(cnt), st)
-            self._dual_ws = table
-        # the cubes with all 8 corners (cnt == 8) are the reference's compacted list; nearly every
-        # centre is one, so the count and emit passes skip the others in place instead of
-        # compacting acc first (same triangles, same order); dual_cubes() compacts on request
-        self.topology_overflow = cnt  # counts above 8 mark the reference's "Topology Error"
-        self._mark("dual grid")
-        # field at the primal samples
-        vals = (self.chi_cells(pos) if n_upsample == 2 else self.chi_raw(pos)) - mean
-        self._mark("chi")
-        verts, faces = self.marching_cubes(acc, cnt, pos, vals, total)
-        self._mark("mesh")
-        self.mesh_info = dict(n_primal=total, n_dual=nd, max_depth=max_depth, acc_ids=acc, cnt=cnt, values=vals,
-                              positions=pos, counts=counts, starts=starts)
-        return verts, faces
-
-    def marching_cubes(self, acc, cnt, pos, vals, n_primal=None):
-        """Dual marching cubes over the complete dual cubes (count 8) and vertex de-duplication by
-        corner-id pair (dual_mc.cu:33-189, reconstructor.py:379-383): vertices [V, 3], faces [F, 3].
-        ``vals`` are the field values at the primal samples ``pos`` (any source: the mesh of a field
-        computed elsewhere goes through the same kernels)."""
-        st, dev = L.stream(), self.dev
-        nd = cnt.shape[0]
-        total = pos.shape[0] if n_primal is None else n_primal
-        vals = vals.contiguous().float()
-        # marching cubes
-        vcount = torch.empty(nd, dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_count", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(vals), L.ptr(vcount), st)
-        voff, vtot = L.scan(vcount)
-        nv = int(vtot.item())
-        tris = torch.empty((nv, 3), dtype=torch.float32, device=dev)
-        vids = torch.empty((nv, 2), dtype=torch.int32, device=dev)
-        L.call("ngs_dual_mc_emit", L.ptr(acc), 1, L.ptr(cnt), nd, L.ptr(pos), L.ptr(vals), L.ptr(voff), L.ptr(tris),
-               L.ptr(vids), st)
-        # vertex de-duplication by (vid0, vid1) (reconstructor.py:380-383)
-        bcount = torch.zeros(total, dtype=torch.int32, device=dev)
-        L.call("ngs_vdedup_count", L.ptr(vids), nv, L.ptr(bcount), st)
-        bstart, _ = L.scan(bcount)
-        fill = torch.zeros(total, dtype=torch.int32, device=dev)
-        sorted_keys = torch.empty(nv, dtype=torch.int64, device=dev)
-        first = torch.empty(nv, dtype=torch.int32, device=dev)
-        L.call("ngs_vdedup_sort", L.ptr(vids), nv, L.ptr(bstart), total, L.ptr(fill), L.ptr(sorted_keys),
-               L.ptr(first), st)
-        vid_of, nvert_t = L.scan(first)
-        nvert = int(nvert_t.item())
-        faces = torch.empty(nv, dtype=torch.int64, device=dev)
-        verts = torch.empty((nvert, 3), dtype=torch.float32, device=dev)
-        L.call("ngs_vdedup_emit", L.ptr(vids), L.ptr(tris), nv, L.ptr(bstart), L.ptr(fill), L.ptr(sorted_keys),
-               L.ptr(vid_of), L.ptr(faces), L.ptr(verts), st)
-        self.mesh_vids = vids          # (larger, smaller) primal-sample pair of every triangle corner
-        return verts, faces.view(-1, 3)
-
-    def dual_cubes(self) -> torch.Tensor:
-        """The complete dual cubes of the last extract_mesh (count 8), in dual-centre order: the
-        reference's compacted [M, 8, 2] (primal id, depth) list (reconstructor.py:366)."""
-        acc, cnt = self.mesh_info["acc_ids"], self.mesh_info["cnt"]
-        nd = cnt.shape[0]
-        st = L.stream()
-        keep = torch.empty(nd, dtype=torch.int32, device=self.dev)
-        L.call("ngs_dual_mc_select", L.ptr(cnt), nd, L.ptr(keep), st)
-        koff, ktot = L.scan(keep)
-        m = int(ktot.item())
-        ids = torch.empty((m, 8), dtype=torch.int32, device=self.dev)
-        L.call("ngs_dual_mc_compact", L.ptr(acc), 1, L.ptr(keep), L.ptr(koff), nd, L.ptr(ids), st)
-        # the depth of a primal sample is the level whose segment holds its id
-        bounds = torch.as_tensor(np.asarray(self.mesh_info["starts"][1:], dtype=np.int64), device=self.dev)
-        depth = torch.bucketize(ids.long(), bounds, right=True).int()
-        return torch.stack([ids, depth], dim=2)
-
-    def _dual_centres_by_sort(self, epb, starts, counts, max_depth, lo, offs):
-        """Unique corners of the expanded cells, in lexicographic order, and a key table over them."""
-        from ..ext import HashLookupData, hash_cuda
-        lo_t = torch.as_tensor(lo, dtype=torch.int64, device=self.dev)
-        keys = []
-        for d in range(max_depth):
-            c = epb[starts[d]:starts[d] + counts[d]]
-            if c.shape[0] == 0:
-                continue
-            corners = (c[:, None, :].long() + offs.long()[None] * self.levels[d].stride).reshape(-1, 3) - lo_t
-            keys.append((corners[:, 0] << 42) | (corners[:, 1] << 21) | corners[:, 2])
-        uk = torch.unique(torch.cat(keys))           # sorted: packed keys order like (x, y, z)
-        mask = (1 << 21) - 1
-        dual = (torch.stack([uk >> 42, (uk >> 21) & mask, uk & mask], 1) + lo_t).int()
-        return int(uk.numel()), HashLookupData(hash_cuda(dual), None, False)
+        field = (lambda pos: self.chi_cells(pos) - mean) if n_upsample == 2 else (lambda pos: self.chi_raw(pos) - mean)
+        return self.mesh_from_leaves(base, max_depth, n_upsample, field)
 
     def run(self, n_upsample: int = 2):
         self.build_tree().assemble().solve()

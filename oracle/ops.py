@@ -307,3 +307,26 @@ def dual_marching_cubes_sparse(acc, corner_pos, corner_val):
     tris, vids = dual_marching_cubes(np.asarray(acc), np.asarray(corner_pos, dtype=np.float64),
                                      np.asarray(corner_val, dtype=np.float64))
     return tris.astype(np.float32), vids
+
+
+# ----------------------------------------------------------------------------- signed distance from points
+def knn(queries, ref_xyz, k):
+    """Exact k nearest reference points (FP64 distances), nearest first: (indices, squared distances).
+    The reference's k-d tree search (``csrc/common/kdtree_cuda.cu:1071-1279``) in scipy's cKDTree."""
+    from scipy.spatial import cKDTree
+    d, idx = cKDTree(np.asarray(ref_xyz, np.float64)).query(np.asarray(queries, np.float64), k=k)
+    return idx.reshape(-1, k), (d ** 2).reshape(-1, k)
+
+
+def sdf_from_points(queries, ref_xyz, ref_normal, nb_points, stdv):
+    """``ext/sdfgen/sdf_from_points.cu:31-68``: magnitude from the nearest point (the distance to its
+    tangent plane when closer than ``stdv``, else the distance to it), sign negative unless more than
+    ``nb_points // 2`` of the nearest normals see the query on their positive side."""
+    q = np.asarray(queries, np.float64)
+    idx, _ = knn(q, ref_xyz, nb_points)
+    ray = q[:, None, :] - np.asarray(ref_xyz, np.float64)[idx]
+    dots = np.sum(np.asarray(ref_normal, np.float64)[idx] * ray, -1)
+    length0 = np.linalg.norm(ray[:, 0], axis=1)
+    mag = np.where(length0 < stdv, np.abs(dots[:, 0]), length0)
+    pos = np.count_nonzero(dots > 0, axis=1)
+    return np.where(pos <= nb_points // 2, -mag, mag), idx
