@@ -260,7 +260,9 @@ def solve_levels(jobs, spec):
         if row[1] not in (L.NGS_OK, L.NGS_ERR_NOT_CONVERGED) or (row[1] == L.NGS_ERR_NOT_CONVERGED and spec.maxiter < 0):
             raise L.NgsError(int(row[1]), f"Galerkin level solve {k}")
     del keep
-    return [o[0] for o in outs], status
+    # the reference mode solves in FP32 throughout and writes only the FP32 solution
+    sols = [o[1].double() if mode == L.PCG_REFERENCE else o[0] for o in outs]
+    return sols, status
 
 
 # ----------------------------------------------------------------------------- forward of one shape, one level

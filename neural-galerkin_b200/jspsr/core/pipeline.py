@@ -419,8 +419,7 @@ class Reconstruction(DualMesher):
             lv.rowptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
             L.scan(counts, out=lv.rowptr[:lv.n], total=lv.rowptr[lv.n:])
         self._mark("structure")
-        # with the non-zero counts, a bound on |column - row| per level: a voxel's stencil spans the x
-        # slabs x-2 .. x+2, whose rows lie between the first rank of slab x-2 and the last of slab x+2
+        # with the non-zero counts, a bound on |column - row| per level (decides the 2-byte columns)
         span = [self._row_span_bound(lv) for lv in self.levels]
         host = torch.stack([lv.rowptr[lv.n] for lv in self.levels] + span).cpu().numpy()
         nnz, span = host[:self.depth], host[self.depth:]
@@ -455,14 +454,21 @@ class Reconstruction(DualMesher):
 
     @staticmethod
     def _row_span_bound(lv: Level) -> torch.Tensor:
-        """Device scalar >= max |column - row| of the level's 5^3-stencil matrix: rows are ranks in
-        (x, y, z) order, so the rows of the stencil of a voxel in x slab i lie in slabs i-2 .. i+2."""
+        """Device scalar >= max |column - row| of the level's 5^3-stencil matrix.  Rows are ranks in
+        (x, y, z) order, so the stencil of a voxel in column (x, y) reaches from the first row of
+        column (x-2, y-2) to the last row of column (x+2, y+2), while the voxel's own row lies within
+        column (x, y): the bound is the larger of the two one-sided spans, read from the first rank of
+        every (x, y) column of the bitmap."""
         g = lv.grid
-        d0, per_slab = int(g.dims[0]), int(g.dims[1]) * int(g.zwords)
-        first = lv.words.view(torch.int32).view(-1, 4)[::per_slab, 0][:d0].long()
+        d0, d1, zw = int(g.dims[0]), int(g.dims[1]), int(g.zwords)
+        first = lv.words.view(torch.int32).view(-1, 4)[::zw, 0][:d0 * d1].long()
         starts = torch.cat([first, torch.full((1,), lv.n, dtype=torch.int64, device=first.device)])
-        i = torch.arange(d0, device=first.device)
-        return (starts[(i + 3).clamp(max=d0)] - starts[(i - 2).clamp(min=0)]).max()
+        x = torch.arange(d0, device=first.device)[:, None]
+        y = torch.arange(d1, device=first.device)[None, :]
+        own = x * d1 + y
+        lo = (x - 2).clamp(min=0) * d1 + (y - 2).clamp(min=0)
+        hi = (x + 2).clamp(max=d0 - 1) * d1 + (y + 2).clamp(max=d1 - 1) + 1
+        return torch.maximum((starts[hi] - starts[own]).max(), (starts[own + 1] - starts[lo]).max())
 
     # ------------------------------------------------------------------ RHS + solve
     def _rhs(self, d):

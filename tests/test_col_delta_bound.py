@@ -1,6 +1,7 @@
 """The bound on |column - row| that decides whether a level's solver reads 2-byte column deltas.
 
-``Reconstruction._row_span_bound`` works from the rank bitmap alone (the first rank of every x slab);
+``Reconstruction._row_span_bound`` works from the rank bitmap alone (the first rank of every (x, y)
+column);
 here it runs on CPU over bitmaps built from the oracle's voxel sets and must cover every entry of
 the oracle's matrices of the same levels.
 """
@@ -47,4 +48,4 @@ def test_row_span_bound_covers_every_column():
         rows = np.repeat(np.arange(coords.shape[0]), np.diff(rp))
         actual = int(np.abs(cols - rows).max())
         assert actual <= bound, (d, actual, bound)
-        assert bound <= 16 * actual + 64, (d, actual, bound)      # and it is not vacuous
+        assert bound <= 1.25 * actual + 64, (d, actual, bound)    # and it is tight enough to use

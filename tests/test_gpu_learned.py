@@ -90,11 +90,13 @@ def test_learned_batch_equals_single_shapes(step):
     fl = [{d: v.detach().clone().requires_grad_(True) for d, v in f.items()} for f in feats]
     total, losses, _ = batch.forward(normals, fl)
     total.backward()
+    # the same systems and solves (a batched solve is bit-identical to a solo one); the FP32 scatter
+    # sums of the assembly run on atomics, whose order varies, hence a 1e-5 tolerance
     for k, (loss, gn, gf, _, _) in enumerate(singles):
-        assert abs(float(losses[k]) - loss) <= 1e-6 * loss, k
-        assert rel(normals[k].grad.cpu().numpy(), gn.cpu().numpy()) < 1e-6, k
+        assert abs(float(losses[k]) - loss) <= 1e-5 * loss, k
+        assert rel(normals[k].grad.cpu().numpy(), gn.cpu().numpy()) < 1e-5, k
         for d in gf:
-            assert rel(fl[k][d].grad.cpu().numpy(), gf[d].cpu().numpy()) < 1e-6, (k, d)
+            assert rel(fl[k][d].grad.cpu().numpy(), gf[d].cpu().numpy()) < 1e-5, (k, d)
 
 
 def _loss64(s, normal, feats):

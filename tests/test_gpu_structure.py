@@ -47,8 +47,8 @@ def test_voxel_status(dense):
 
 def test_expanded_and_conforming_coords(dense):
     for d in range(3):
-        assert np.array_equal(dense._enc_branch.get_coords(d, expand=3).cpu().numpy(), G[f"expand{d}"]), d
-        assert np.array_equal(dense._enc_branch.get_coords(d, conforming=True).cpu().numpy(), G[f"conform{d}"]), d
+        assert np.array_equal(dense._get_branch(dense.ENCODER).get_coords(d, expand=3).cpu().numpy(), G[f"expand{d}"]), d
+        assert np.array_equal(dense._get_branch(dense.ENCODER).get_coords(d, conforming=True).cpu().numpy(), G[f"conform{d}"]), d
 
 
 def test_split_data_and_test_grid(dense):

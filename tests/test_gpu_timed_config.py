@@ -69,6 +69,7 @@ def check_parity(ref, rec, v, f, depth, report):
     report["sign_flips"] = flips
     report["samples"] = int(vals.size)
     assert e_f <= TOL, e_f
+    own_vids = rec.mesh_vids.cpu().numpy().astype(np.int64)       # the GPU mesh's own vertex pairs
     # topology: the oracle's field through the production marching cubes
     cubes = rec.dual_cubes()[:, :, 0].cpu().numpy()
     np.testing.assert_array_equal(cubes, ref["cubes"])
@@ -77,7 +78,7 @@ def check_parity(ref, rec, v, f, depth, report):
     np.testing.assert_array_equal(f_o.cpu().numpy(), ref["faces"])
     report["faces_from_oracle_field_equal"] = True
     # vertices of the GPU's own mesh against the oracle's, matched by primal-sample pair
-    vids = rec.mesh_vids.cpu().numpy().astype(np.int64)
+    vids = own_vids
     keys = np.empty(v.shape[0], np.int64)
     keys[f.reshape(-1)] = (vids[:, 0] << 32) | vids[:, 1]
     common, ia, ib = np.intersect1d(keys, ref["vertex_keys"], assume_unique=True, return_indices=True)
