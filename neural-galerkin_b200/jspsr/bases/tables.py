@@ -4,8 +4,8 @@ The reference ships these as ``jspsr/data/bezier_integrals.pkl``
 (``jspsr/bases/bezier_tensor.py:26-34``), a file that was never published.  The
 tables follow from the basis definition (``bezier_tensor.py:17-22``) and the
 index conventions of ``bezier_tensor.py:75-121``; every entry is the integral
-of a piecewise polynomial, evaluated here exactly (antiderivatives of the
-polynomial pieces between consecutive knots).  Level ratios beyond the
+of a piecewise polynomial, evaluated here in closed form (antiderivatives of the
+polynomial pieces between consecutive knots, in a variable local to each interval).  Level ratios beyond the
 reference's 16 (``n_multiples=5``) follow from the same formulas.
 
 Names and meaning (M = 2**m is the stride ratio of the two levels):
@@ -30,30 +30,43 @@ _PIECES = (np.array([2.25, 3.0, 1.0]), np.array([1.5, 0.0, -2.0]), np.array([2.2
 
 
 def _piece(x_lo, x_hi, scale=1.0, shift=0.0, deriv=False):
-    """Pieces of B(scale * y + shift) (or d/du B(u) at u = scale*y + shift) as polynomials in y."""
+    """Pieces of B(scale * y + shift) (or d/du B(u) at u = scale*y + shift) on the y line: each piece is
+    (y_lo, y_hi, polynomial in u, scale, shift).  The polynomial stays in the spline's own variable u,
+    whose range is the knot span: integrals are taken in a variable local to each interval, never by
+    evaluating antiderivatives at large y (at a level ratio M = 1024 the y range reaches 1.5M, and an
+    antiderivative expanded in y loses every digit of the small entries to cancellation)."""
     out = []
     for (a, b), c in zip(zip(_KNOTS[:-1], _KNOTS[1:]), _PIECES):
         poly = P.polyder(c) if deriv else c
-        # u = scale * y + shift  ->  y in [(a - shift) / scale, (b - shift) / scale]
-        lo, hi = (a - shift) / scale, (b - shift) / scale
-        comp = np.zeros(1)
-        for k, ck in enumerate(poly):
-            comp = P.polyadd(comp, ck * P.polypow([shift, scale], k))
-        out.append((lo, hi, comp))
+        out.append(((a - shift) / scale, (b - shift) / scale, poly, scale, shift))
     return out
+
+
+def _local(piece, y0):
+    """The piece as a polynomial in t = y - y0 (u = scale * y0 + shift + scale * t)."""
+    _, _, poly, scale, shift = piece
+    u0 = scale * y0 + shift
+    comp = np.zeros(1)
+    for k, ck in enumerate(poly):
+        comp = P.polyadd(comp, ck * P.polypow([u0, scale], k))
+    return comp
+
+
+_ONE = ((-np.inf, np.inf, np.array([1.0]), 1.0, 0.0),)
 
 
 def _integrate_product(f_pieces, g_pieces=None, lo=-np.inf, hi=np.inf):
     total = 0.0
     if g_pieces is None:
-        g_pieces = [(-np.inf, np.inf, np.array([1.0]))]
-    for fl, fh, fp in f_pieces:
-        for gl, gh, gp in g_pieces:
-            a, b = max(fl, gl, lo), min(fh, gh, hi)
+        g_pieces = _ONE
+    for fpc in f_pieces:
+        for gpc in g_pieces:
+            a, b = max(fpc[0], gpc[0], lo), min(fpc[1], gpc[1], hi)
             if b <= a:
                 continue
-            anti = P.polyint(P.polymul(fp, gp))
-            total += P.polyval(b, anti) - P.polyval(a, anti)
+            # integrate over t = y - a in [0, b - a]
+            anti = P.polyint(P.polymul(_local(fpc, a), _local(gpc, a)))
+            total += P.polyval(b - a, anti)
     return total
 
 

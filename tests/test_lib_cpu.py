@@ -89,6 +89,27 @@ def test_product_tables_match_oracle():
             np.testing.assert_allclose(g, t["INV_PARTIAL_INTEGRAL"][m - 1], atol=1e-11)
 
 
+def test_product_tables_beyond_reference_ratios():
+    """Level ratios 32 .. 1024 (m = 5 .. 10), outside the reference's tables (n_multiples = 5), used by
+    hierarchies deeper than 5 levels: every entry against the oracle's piecewise Gauss-Legendre
+    quadrature (exact for the polynomial pieces), relative to the entry itself.  The smallest
+    entries at m = 10 are ~3e-8 while the integration range spans 1.5 * 1024 voxels."""
+    import numpy as np
+    from jspsr.bases import tables as P
+    from oracle import tables as T
+    t = T.bezier_tables(11)
+    for m in range(5, 11):
+        s, d = P.shifted(m)
+        np.testing.assert_allclose(s, t["SHIFTED_SELF_INTEGRAL"][m], rtol=1e-11, atol=1e-22, err_msg=f"m={m}")
+        np.testing.assert_allclose(d, t["SHIFTED_DERIVATIVE_INTEGRAL"][m], rtol=1e-11, atol=1e-14, err_msg=f"m={m}")
+        f, g = P.partial(m)
+        np.testing.assert_allclose(f, t["DERIVATIVE_PARTIAL_INTEGRAL"][m], rtol=1e-11, atol=1e-14)
+        np.testing.assert_allclose(g, t["PARTIAL_INTEGRAL"][m], rtol=1e-11, atol=1e-14)
+        f, g = P.inverse_partial(m)
+        np.testing.assert_allclose(f, t["INV_DERIVATIVE_PARTIAL_INTEGRAL"][m - 1], atol=1e-14)
+        np.testing.assert_allclose(g, t["INV_PARTIAL_INTEGRAL"][m - 1], atol=1e-14)
+
+
 def test_stencil_is_symmetric_and_annihilates_nothing():
     import numpy as np
     from jspsr.bases import tables as P
