@@ -232,6 +232,72 @@ def learned_leg(n_shapes=32):
                       "32 shapes in one batched Galerkin solve"}
 
 
+# ----------------------------------------------------------------------------- sparse convolution leg
+def conv_leg(cin=64, cout=64, reps=10):
+    """One 3^3 sparse convolution layer (the Neural Galerkin U-Net's building block) on the finest voxel
+    level of the benchmark cloud: forward, input gradient and weight gradient in bf16 with FP32
+    accumulation on the tensor cores, device time per pass (mean of ``reps`` after warm-up), against
+    the reference's algorithm in torch (per offset: gather, GEMM, scatter-add) on the same data."""
+    import torch
+    from jspsr import ext
+    from jspsr.core._hash_backend import VoxelLevel
+    from jspsr.core.pipeline import Reconstruction
+    xyz, nrm = workload_points()
+    W = WORKLOAD
+    rec = Reconstruction(torch.from_numpy(xyz).cuda(), torch.from_numpy(nrm).cuda(), W["voxel_size"], W["depth"],
+                         W["min_density"], W["screen_alpha"], solver=W["solver"])
+    rec.build_tree()
+    coords = rec.levels[0].coords
+    lv = VoxelLevel(coords, 1)
+    ax = torch.arange(-1, 2)
+    offs = torch.cartesian_prod(ax, ax, ax).to(torch.int32).cuda()
+    src, tgt, kidx, counts = lv.neighbours(coords, 1, offs, True, False)
+    nbmaps = torch.stack([tgt, src], 1).int().contiguous()     # (input row, output row) per offset
+    nbsizes = counts.int().cpu()
+    n = coords.shape[0]
+    pairs = int(nbsizes.sum())
+    gen = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.randn(n, cin, generator=gen).cuda().bfloat16()
+    w = (torch.randn(27, cin, cout, generator=gen) / cin ** 0.5).cuda().bfloat16()
+    gy = torch.randn(n, cout, generator=gen).cuda().bfloat16()
+    out = torch.zeros(n, cout, dtype=torch.bfloat16, device="cuda")
+    gx = torch.zeros_like(x)
+    gw = torch.zeros_like(w)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e[0].record()
+        for _ in range(reps):
+            fn()
+        e[1].record()
+        torch.cuda.synchronize()
+        return e[0].elapsed_time(e[1]) / reps
+
+    fwd = timed(lambda: ext.sparse_op.convolution_forward_cuda(x, out, w, nbmaps, nbsizes, False, False))
+    bwd = timed(lambda: ext.sparse_op.convolution_backward_cuda(x, gx, gy, w, gw, nbmaps, nbsizes, False))
+    starts = np.concatenate([[0], np.cumsum(nbsizes.numpy())])
+
+    def reference_forward():
+        res = x[:, :0].new_zeros(n, cout)
+        for k in range(27):
+            a, b = int(starts[k]), int(starts[k + 1])
+            res.index_add_(0, nbmaps[a:b, 1].long(), torch.mm(x[nbmaps[a:b, 0].long()], w[k]))
+        return res
+    ref_fwd = timed(reference_forward)
+    flops = 2.0 * pairs * cin * cout
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops", 1590.0)
+    return {"voxels": n, "pairs": pairs, "cin": cin, "cout": cout, "dtype": "bf16 in, fp32 accumulate",
+            "forward_ms": fwd, "backward_ms": bwd, "forward_tflops": flops / fwd / 1e9,
+            "backward_tflops": 2 * flops / bwd / 1e9, "peak_bf16_tflops": peak,
+            "forward_frac_of_peak": flops / fwd / 1e9 / peak,
+            "reference_algorithm_torch_forward_ms": ref_fwd, "forward_speedup_vs_reference_algorithm": ref_fwd / fwd,
+            "config": "3^3 kernel over the finest voxel level of the benchmark cloud, the U-Net's 64 -> 64 layer"}
+
+
 # ----------------------------------------------------------------------------- serving leg
 def serving_leg(n_requests=1024, slots=8, plain_every=8):
     """1,024 requests (points log-uniform in [1e3, 5e5], superquadric/torus unions, N(0,0.003) noise,
@@ -307,7 +373,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-comparators", action="store_true")
     ap.add_argument("--workload", default="superquadrics-300k", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="all", choices=["all", "recon", "learned", "serving", "profile"],
+    ap.add_argument("--mode", default="all", choices=["all", "recon", "learned", "serving", "conv", "profile"],
                     help="all: reconstruction line with the learned-basis and serving legs attached; profile: "
                          "warm-up reconstructions, then one between cudaProfilerStart/Stop (for ncu "
                          "--profile-from-start off)")
@@ -336,9 +402,9 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     lib = L.load()
-    if args.mode in ("learned", "serving"):
+    if args.mode in ("learned", "serving", "conv"):
         leg = learned_leg(args.learned_shapes) if args.mode == "learned" else \
-            serving_leg(args.serving_requests, slots=args.serving_slots)
+            conv_leg() if args.mode == "conv" else serving_leg(args.serving_requests, slots=args.serving_slots)
         if rank == 0:
             print(json.dumps({"mode": args.mode, **leg}), flush=True)
         if world > 1:
@@ -349,8 +415,9 @@ def main():
     N = torch.from_numpy(nrm).cuda()
     W = WORKLOAD
 
-    def step(solver=W["solver"], profile=False):
-        rec = Reconstruction(X, N, W["voxel_size"], W["depth"], W["min_density"], W["screen_alpha"], solver=solver)
+    def step(solver=W["solver"], profile=False, operator="csr"):
+        rec = Reconstruction(X, N, W["voxel_size"], W["depth"], W["min_density"], W["screen_alpha"], solver=solver,
+                             operator=operator)
         rec.profile_pcg = profile
         v, f = rec.run()
         return rec, v, f
@@ -456,6 +523,11 @@ def main():
         step(solver=FP64_SOLVER)         # warm-up of the FP64 kernel, as above
         fp64_rec, _, _ = step(solver=FP64_SOLVER, profile=True)
         fp64_solve = fp64_rec.pcg_ms
+        # the matrix-free operator (stencil over the bitmap + point form of the screening) on the
+        # levels where it applies, same solver
+        step(operator="matrix-free")
+        mf_rec, _, _ = step(profile=True, operator="matrix-free")
+        mf_solve = mf_rec.pcg_ms
         # errors against every level solved to 1e-12 in FP64 on the GPU: field at the input points,
         # solutions, and mesh vertices matched by their primal-sample pair
         ref64, v64, f64 = step(solver=EXACT_SOLVER)
@@ -478,7 +550,10 @@ def main():
         mixed_solve = sum(pcg_ms.values())
         extra = {"plain_fp64_ms_per_step": plain_ms, "speedup_vs_plain_fp64": plain_ms / (ms / args.steps),
                  "solve_ms": {"mixed": mixed_solve, "plain_fp64_host_driven": sum(plain_solve.values()),
-                              "fp64_persistent_same_tol": sum(fp64_solve.values())},
+                              "fp64_persistent_same_tol": sum(fp64_solve.values()),
+                              "mixed_matrix_free_operator": sum(mf_solve.values())},
+                 "matrix_free_levels": [d for d, lv in enumerate(mf_rec.levels) if lv.mf],
+                 "matrix_free_pcg_ms_per_level": mf_solve,
                  "solve_speedup_vs_plain_fp64": sum(plain_solve.values()) / mixed_solve,
                  "solve_speedup_vs_fp64_persistent": sum(fp64_solve.values()) / mixed_solve,
                  "error_vs_fp64_exact": {"reference": EXACT_SOLVER, "field": err, "solution": xerr, "vertices": verr,
@@ -493,6 +568,7 @@ def main():
     # ---------------------------------------------------------------- learned-basis and serving legs
     if args.mode == "all" and rank == 0 and world == 1:
         extra["learned"] = learned_leg(args.learned_shapes)
+        extra["sparse_conv"] = conv_leg()
         extra["serving"] = serving_leg(args.serving_requests, slots=args.serving_slots)
 
     # ---------------------------------------------------------------- CPU baseline (the reference path on the host)

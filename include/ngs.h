@@ -279,6 +279,32 @@ int ngs_finish_system(const double* vals64, int64_t nnz, const int64_t* diag_slo
  *   NGS_PCG_FP64       all-FP64 Jacobi-PCG (vals64, b64), device-side loop.        */
 enum { NGS_PCG_REFERENCE = 0, NGS_PCG_MIXED = 1, NGS_PCG_FP64 = 2 };
 
+/* Matrix-free operator of one level of the B-spline system (no counterpart in the reference, whose
+ * solve multiplies an assembled CSR: csrc/sparse_solve/solve_pcg.cu:67-73, assembled at
+ * jspsr/core/reconstructor.py:176-185):
+ *     A = K (*) v  +  alpha * Phi^T (Phi v)
+ * K: the level's 5x5x5 stiffness stencil (125 FP64 values, offsets (dx, dy, dz) in [-2, 2]^3 in
+ * lexicographic order), applied over the level's rank bitmap; Phi: the point basis, [N, 27] rows
+ * (-1: absent) and values, and the same pairs transposed per row (t_ptr [n+1], t_point / t_phi [E],
+ * ascending point index within a row).  scratch32 / scratch64: [N] per-point products (MIXED uses
+ * both, FP64 the second).  Used by ngs_pcg_solve / ngs_pcg_solve_batch (MIXED and FP64 modes) when
+ * ngs_pcg_system.op is set; the solver then reads no CSR (rowptr, cols, vals32/64 may be NULL) and
+ * `nnz` carries the operator's work per application (60 * n + 2 * E) for the block count. */
+typedef struct ngs_pcg_operator {
+  ngs_grid grid;
+  const int32_t* coords;     /* [n, 3] voxel coordinates (finest-voxel units) */
+  const double* stencil;     /* [125] */
+  double alpha;              /* screening weight of the level */
+  int64_t n_points;
+  const int32_t* point_rows; /* [N, 27] */
+  const float* point_phi;    /* [N, 27] */
+  const int64_t* t_ptr;      /* [n + 1] */
+  const int32_t* t_point;    /* [E] */
+  const float* t_phi;        /* [E] */
+  float* scratch32;          /* [N] */
+  double* scratch64;         /* [N] */
+} ngs_pcg_operator;
+
 typedef struct ngs_pcg_system {
   int64_t n;
   int64_t nnz;
@@ -293,6 +319,7 @@ typedef struct ngs_pcg_system {
   double* x64;               /* [n] out (MIXED, FP64) */
   const int16_t* col_delta;  /* [nnz] optional: column - row of every entry; when given the solver
                                 reads these 2-byte deltas instead of the 4-byte columns (NULL: cols) */
+  const ngs_pcg_operator* op;/* optional: matrix-free operator instead of the CSR (NULL: CSR) */
 } ngs_pcg_system;
 
 typedef struct ngs_pcg_config {
@@ -350,10 +377,62 @@ int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items, ngs_stream
  * their own copy; the first call in each context loads the library's device code there -- make
  * that first call before any stream capture.  All calls in the process share the one array: calls that may overlap on the GPU
  * (different streams, or concurrent host threads) race and must be serialised by the caller.
- * Nothing is allocated: no cudaMalloc / cudaFree, no allocating library routine. */
+ * Nothing is allocated: no cudaMalloc / cudaFree, no allocating library routine.  Assembled (CSR)
+ * systems only: a system with a matrix-free operator (sys->op) returns NGS_ERR_INVALID_ARG. */
 int64_t ngs_pcg_noalloc_max_rows(void);
 int ngs_pcg_solve_noalloc(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, int64_t* info_dev,
                           double* resid_dev, ngs_stream s);
+
+/* Builders of the matrix-free operator (ngs_pcg_operator; no counterpart in the reference, which
+ * assembles the screening Gram into its LHS: jspsr/core/reconstructor.py:181-185 over
+ * csrc/sparse_op/sparse_product.cu:100-137).
+ * ngs_mf_count: counts[V] (zeroed by the caller) += present (point, slot) pairs per row, max_dev[0]
+ *   (zeroed) = the largest count.
+ * ngs_mf_fill: the transposed pairs, ascending point index within each row (t_ptr = exclusive scan
+ *   of the counts, cursor[V] zeroed scratch, tmp_point / tmp_phi [E] scratch).
+ * ngs_mf_diag: inv_diag[i] = 1 / (stencil_center + alpha * sum phi^2) (FP64 sum, FP32 result).
+ * ngs_mf_screen_rhs: rhs[i] += scale * sum over the row's pairs of phi * (val ? val[point] : 1).
+ * ngs_mf_apply64: y = A x in FP64 (t64: [N] scratch); two launches. */
+int ngs_mf_count(const int32_t* point_rows, int64_t n_points, int64_t V, int32_t* counts, int32_t* max_dev,
+                 ngs_stream s);
+int ngs_mf_fill(const int32_t* point_rows, const float* point_phi, int64_t n_points, const int64_t* t_ptr, int64_t V,
+                int32_t* cursor, int32_t* tmp_point, float* tmp_phi, int32_t* t_point, float* t_phi, ngs_stream s);
+int ngs_mf_diag(const int64_t* t_ptr, const float* t_phi, int64_t V, double stencil_center, double alpha,
+                float* inv_diag, ngs_stream s);
+int ngs_mf_screen_rhs(const int64_t* t_ptr, const int32_t* t_point, const float* t_phi, int64_t V, const float* val,
+                      double scale, double* rhs, ngs_stream s);
+int ngs_mf_apply64(const ngs_pcg_operator* op, int64_t n, const double* x, double* y, ngs_stream s);
+
+/* ======================================================================= sparse convolution
+ * ref: csrc/sparse_op/convolution_cuda.cu:52-174 (convolution_forward_cuda), :176-282
+ * (convolution_backward_cuda), called by models/ascn/utils.py:108-190 (ConvolutionFunction).
+ * Feature types: NGS_F16 / NGS_BF16 run on the tensor cores (tcgen05.mma, FP32 accumulation),
+ * NGS_F32 on the CUDA cores in FP32 (as the reference's FP32 cuBLAS path).
+ * ngs_conv_table: table[row, k] (int32 [n_rows, K], filled here) = the row paired with `row` at offset
+ *   k in nbmaps (int32 [P, 2], the pairs of offset k at starts[k] .. starts[k+1], starts int64 [K+1] on
+ *   the device), -1 for none; key_col is the column of nbmaps that indexes the table; mid >= 0 sets
+ *   table[row, mid] = row (the reference's forward takes the centre offset as the identity when the
+ *   input and output sets are the same).
+ * ngs_conv_gather_gemm: out[r, n] = sum_k sum_c x[table[r, k], c] * bt[k, n, c] (bt = the weights of
+ *   every offset with the reduction index innermost), one kernel, every output row written once
+ *   (FP32 out when out_f32, else the input type).  Forward: x = input, bt = W^T per offset
+ *   (ngs_conv_transpose_weight); input gradient: x = output gradient, table of the other column,
+ *   bt = W as stored.
+ * ngs_conv_weight_grad: grad_w[k, i, o] = sum over the pairs (in, out) of offset k of x[in, i] * gy[out, o]
+ *   (in_col: the nbmaps column of the input rows); splits of the pairs summed in a fixed order through
+ *   ws (ngs_conv_weight_grad_ws_bytes; max_pairs = the largest per-offset pair count).
+ * error_dev (int, zeroed by the caller): NGS_ERR_TIMEOUT if a bounded device wait ran out. */
+enum { NGS_F16 = 0, NGS_BF16 = 1, NGS_F32 = 2 };
+int ngs_conv_table(const int32_t* nbmaps, const int64_t* starts_dev, int K, int key_col, int64_t n_rows, int mid,
+                   int32_t* table, ngs_stream s);
+int ngs_conv_transpose_weight(const void* w, int K, int a, int b, int dtype, void* wt, ngs_stream s);
+int ngs_conv_tensor_core_ok(int kdim, int ncols, int dtype);
+int ngs_conv_gather_gemm(const void* x, int64_t n_src, int kdim, const int32_t* table, int64_t n_rows, int K,
+                         const void* bt, int ncols, int dtype, void* out, int out_f32, int* error_dev, ngs_stream s);
+size_t ngs_conv_weight_grad_ws_bytes(int K, int cin, int cout, int64_t max_pairs);
+int ngs_conv_weight_grad(const void* x, int64_t n_in, int cin, const void* gy, int64_t n_out, int cout,
+                         const int32_t* nbmaps, const int64_t* starts_dev, int K, int64_t max_pairs, int in_col,
+                         int dtype, void* grad_w, int out_f32, void* ws, size_t ws_bytes, int* error_dev, ngs_stream s);
 
 /* Plain building blocks for the host-driven FP64 comparator (one launch each). */
 int ngs_spmv64(int64_t n, const int64_t* rowptr, const int32_t* cols, const double* vals, const double* x,

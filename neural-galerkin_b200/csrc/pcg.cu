@@ -34,8 +34,9 @@
 // This file is compiled without multiply-add contraction (build.py): the solver body is inlined
 // into the single-system and the batched kernel, and only uncontracted arithmetic is guaranteed to
 // round the same way in both, which makes a batched solve bit-identical to the solo one.
+#include <algorithm>
 #include <cmath>
-#include "ngs_common.cuh"
+#include "mf.cuh"
 
 constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_BLOCKS = 2;      // blocks per SM the register budget is sized for
@@ -81,7 +82,17 @@ struct PcgArgs {
   unsigned long long budget_ns;   // time budget of the whole solve
   unsigned int nblocks;
   int evict_first;                // stream the matrix past the caches (it does not fit L2)
+  int mf;                         // the matrix-free operator below replaces the CSR
+  ngs_pcg_operator op;
+  int win_cap;                    // elements of the search vector a block can stage in shared memory
 };
+
+// Shared memory (dynamic) of every PCG block for its window of the search vector: the SpMV of a
+// block's rows gathers from the contiguous range of rows that its columns span (rows are ranks in
+// (x, y, z) order, so a block's 5x5x5 stencils reach a band of neighbouring x slabs), loaded once per
+// iteration with coalesced loads.  Gathers from L1 cost one wavefront per distinct cache line of the
+// warp (the ~60 columns of a row lie in 25 different z columns); from shared memory a few at most.
+constexpr int PCG_WIN_BYTES = 96 * 1024;
 
 constexpr int NGS_PCG_ITER_CAP = 20000;
 
@@ -109,6 +120,11 @@ NGS_DEV int64_t first_row_at(const int64_t* __restrict__ rp, int64_t n, int64_t 
 NGS_DEV bool block_rows(const PcgArgs& a, unsigned bid, int64_t& row0, int64_t& row1) {
   __shared__ int64_t bounds[2];
   __shared__ int bad;
+  if (a.mf) {                   // matrix-free: every row costs about the same; equal row ranges
+    row0 = (a.n * (int64_t)bid) / a.nblocks;
+    row1 = (a.n * ((int64_t)bid + 1)) / a.nblocks;
+    return true;
+  }
   if (threadIdx.x == 0) {
     const int64_t B = a.nblocks;
     bounds[0] = first_row_at(a.rowptr, a.n, (a.nnz * (int64_t)bid) / B);
@@ -136,8 +152,8 @@ NGS_DEV T ld_mat(const T* p) {
 // The gathered vector is read with plain loads: it was written earlier in this launch.  Ends with a
 // block barrier, after which every thread may read the rows written by the epilogue.
 template <bool STREAM, bool DELTA, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
-NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
-                         Pre pre, Epi epi, double& dsum) {
+NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
+                         int64_t row1, Pre pre, Epi epi, double& dsum) {
   constexpr int L = PCG_ROW_LANES;
   const int sub = threadIdx.x & (L - 1);
   const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
@@ -163,7 +179,7 @@ NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT
       }
       VT xv[U];
 #pragma unroll
-      for (int k = 0; k < U; k++) xv[k] = v[c[k]];
+      for (int k = 0; k < U; k++) xv[k] = v[c[k] - voff];
       // the round's products summed in the matrix type (two chains), the round sum accumulated in ACC:
       // one conversion per round instead of two per product; the FP64 refinement of the mixed mode
       // works from the true residual, so this rounding only shapes the inner iterations
@@ -185,16 +201,41 @@ NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT
 // The streaming choice is a template argument: one load form per instantiation (a runtime choice
 // per load cost 7 % of the level-0 solve and forced register spills).
 template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
-NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t row0, int64_t row1,
-                       Pre pre, Epi epi, double& dsum) {
+NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
+                       int64_t row1, Pre pre, Epi epi, double& dsum) {
   // the column encoding too: 2-byte deltas when the caller supplied them, 4-byte columns otherwise
   if (a.cols16) {
-    if (a.evict_first) spmv_rows_t<true, true, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
-    else spmv_rows_t<false, true, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+    if (a.evict_first) spmv_rows_t<true, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+    else spmv_rows_t<false, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
   } else {
-    if (a.evict_first) spmv_rows_t<true, false, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
-    else spmv_rows_t<false, false, MT, VT, ACC>(a, vals, v, row0, row1, pre, epi, dsum);
+    if (a.evict_first) spmv_rows_t<true, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+    else spmv_rows_t<false, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
   }
+}
+
+// The range of columns [wlo, whi) that the rows [row0, row1) reach (columns are sorted within a row:
+// its first and last entries bound it), into shared memory.  Block-wide.
+NGS_DEV void csr_window(const PcgArgs& a, int64_t row0, int64_t row1, unsigned long long& wlo,
+                        unsigned long long& whi) {
+  if (threadIdx.x == 0) {
+    wlo = ~0ull;
+    whi = 0ull;
+  }
+  __syncthreads();
+  unsigned long long mlo = ~0ull, mhi = 0ull;
+  for (int64_t r = row0 + threadIdx.x; r < row1; r += blockDim.x) {
+    const int64_t e0 = a.rowptr[r], e1 = a.rowptr[r + 1];
+    if (e1 <= e0) continue;
+    const int64_t c0 = a.cols16 ? r + a.cols16[e0] : a.cols[e0];
+    const int64_t c1 = a.cols16 ? r + a.cols16[e1 - 1] : a.cols[e1 - 1];
+    mlo = min(mlo, (unsigned long long)c0);
+    mhi = max(mhi, (unsigned long long)(c1 + 1));
+  }
+  if (mlo != ~0ull) atomicMin(&wlo, mlo);
+  if (mhi != 0ull) atomicMax(&whi, mhi);
+  __syncthreads();
+  if (threadIdx.x == 0 && wlo == ~0ull) wlo = whi = 0ull;
+  __syncthreads();
 }
 
 // Grid synchronisation of a cooperative launch through one arrival counter in global memory (zeroed
@@ -400,7 +441,12 @@ NGS_DEV void pcg_abandon(const PcgArgs& a, int it) {
 
 // The solve of one system by the blocks bid = 0 .. a.nblocks-1 of a launch (all of them for a
 // single solve, a contiguous range for one system of a batch, the CTAs of one cluster).
-template <int MODE, typename Sync>
+// OPS: which operators the instantiation carries -- PCG_OPS_CSR, PCG_OPS_MF, or both (chosen per system
+// at run time; the batched kernel when a batch mixes them).  Single-operator instantiations keep the
+// register budget of the other operator's code out of the kernel.
+constexpr int PCG_OPS_CSR = 1, PCG_OPS_MF = 2, PCG_OPS_BOTH = 3;
+
+template <int MODE, int OPS, typename Sync>
 NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   using MT = typename PcgTypes<MODE>::MT;
   using VT = typename PcgTypes<MODE>::VT;
@@ -436,10 +482,88 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   };
   // the true residual uses the FP64 matrix in MIXED mode, the recurrence matrix otherwise
   auto spmv_true = [&](double& sum) {
-    if constexpr (MODE == NGS_PCG_MIXED) spmv_rows<double, RT, double>(a, a.vals64, x, row0, row1, res_pre, true_res_epi, sum);
-    else spmv_rows<MT, RT, ACC>(a, vals, x, row0, row1, res_pre, true_res_epi, sum);
+    if constexpr (MODE == NGS_PCG_MIXED) spmv_rows<double, RT, double>(a, a.vals64, x, 0, row0, row1, res_pre, true_res_epi, sum);
+    else spmv_rows<MT, RT, ACC>(a, vals, x, 0, row0, row1, res_pre, true_res_epi, sum);
   };
-  auto spmv_w = [&](double& sum) { spmv_rows<MT, VT, ACC>(a, vals, u, row0, row1, w_pre, w_epi, sum); };
+  // w = A u: the block's window of u staged in shared memory when it fits (refreshed every product;
+  // the grid barrier before the product made every block's u rows visible)
+  // (the window bounds stay in shared memory, not in registers across the solve)
+  extern __shared__ __align__(16) unsigned char pcg_win_raw[];
+  __shared__ unsigned long long win_bounds[2];
+  if (threadIdx.x == 0) win_bounds[0] = win_bounds[1] = 0ull;
+  __syncthreads();
+  if constexpr (OPS & PCG_OPS_CSR) {
+    if (!a.mf && rows_ok && a.win_cap > 0) csr_window(a, row0, row1, win_bounds[0], win_bounds[1]);
+  }
+  auto spmv_w = [&](double& sum) {
+    const int64_t wlo = (int64_t)win_bounds[0], wn = (int64_t)win_bounds[1] - wlo;
+    if (wn > 0 && wn <= a.win_cap) {
+      VT* win = reinterpret_cast<VT*>(pcg_win_raw);
+      for (int64_t i = threadIdx.x; i < wn; i += PCG_THREADS) win[i] = u[wlo + i];
+      __syncthreads();
+      spmv_rows<MT, VT, ACC>(a, vals, win, wlo, row0, row1, w_pre, w_epi, sum);
+    } else {
+      spmv_rows<MT, VT, ACC>(a, vals, u, 0, row0, row1, w_pre, w_epi, sum);
+    }
+  };
+
+  // Matrix-free operator (mf.cuh): the stencil in shared memory (FP32 for the inner products of the
+  // mixed mode, FP64 for its true residual and for the FP64 mode), the points split evenly over the
+  // blocks.  An application is two passes with a barrier between them: t = Phi v over the block's
+  // points, then the block's rows.  Returns false if the barrier gave up.
+  __shared__ float ks32[125];
+  __shared__ double ks64[125];
+  int64_t pt0 = 0, pt1 = 0;
+  if ((OPS & PCG_OPS_MF) && a.mf) {
+    for (int k = threadIdx.x; k < 125; k += PCG_THREADS) {
+      ks64[k] = a.op.stencil[k];
+      ks32[k] = (float)a.op.stencil[k];
+    }
+    pt0 = (a.op.n_points * (int64_t)bid) / a.nblocks;
+    pt1 = (a.op.n_points * ((int64_t)bid + 1)) / a.nblocks;
+    __syncthreads();
+  }
+  auto mf_w = [&](double& sum) -> bool {
+    if constexpr (MODE == NGS_PCG_REFERENCE) {
+      return false;                                   // not offered in this mode (rejected on the host)
+    } else {
+      using TT = VT;
+      TT* t = MODE == NGS_PCG_FP64 ? reinterpret_cast<TT*>(a.op.scratch64) : reinterpret_cast<TT*>(a.op.scratch32);
+      mf_points<VT, TT>(a.op, u, t, pt0 + threadIdx.x, pt1, PCG_THREADS);
+      if (!sy.barrier()) return false;
+      const MT* ks = MODE == NGS_PCG_FP64 ? reinterpret_cast<const MT*>(ks64) : reinterpret_cast<const MT*>(ks32);
+      for (int64_t i = i0; i < i1; i += is) sum += w_epi(i, (double)mf_row<MT, VT, TT, ACC>(a.op, ks, u, t, i), w_pre(i));
+      __syncthreads();
+      return true;
+    }
+  };
+  auto mf_true = [&](double& sum) -> bool {
+    if constexpr (MODE == NGS_PCG_REFERENCE) {
+      return false;
+    } else {
+      mf_points<RT, double>(a.op, x, a.op.scratch64, pt0 + threadIdx.x, pt1, PCG_THREADS);
+      if (!sy.barrier()) return false;
+      for (int64_t i = i0; i < i1; i += is)
+        sum += true_res_epi(i, mf_row<double, RT, double, double>(a.op, ks64, x, a.op.scratch64, i), res_pre(i));
+      __syncthreads();
+      return true;
+    }
+  };
+  // w = A u / r = b - A x through whichever operator the system has; false: a barrier gave up
+  auto apply_w = [&](double& sum) -> bool {
+    if constexpr (OPS & PCG_OPS_MF) {
+      if (OPS == PCG_OPS_MF || a.mf) return mf_w(sum);
+    }
+    if constexpr (OPS & PCG_OPS_CSR) spmv_w(sum);
+    return true;
+  };
+  auto apply_true = [&](double& sum) -> bool {
+    if constexpr (OPS & PCG_OPS_MF) {
+      if (OPS == PCG_OPS_MF || a.mf) return mf_true(sum);
+    }
+    if constexpr (OPS & PCG_OPS_CSR) spmv_true(sum);
+    return true;
+  };
 
   // init: x = 0, r = b, u = M r, p = s = 0; partial (b, b); part[1] flags empty rows
   double part[3] = {0.0, rows_ok ? 0.0 : 1.0, 0.0}, res[3];
@@ -461,7 +585,7 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   const double bnorm = sqrt(res[0]);
   const double atol = a.tol * bnorm;
   part[0] = part[1] = part[2] = 0.0;
-  spmv_w(part[1]);
+  if (!apply_w(part[1])) return pcg_abandon(a, it);
   for (int64_t i = i0; i < i1; i += is) {
     part[0] += (double)r[i] * (double)u[i];
     part[2] += (double)r[i] * (double)r[i];
@@ -500,14 +624,14 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
       // residual replacement: r = b - A x (FP64 matrix in MIXED mode, the FP32 one in REFERENCE mode)
       if (!sy.barrier()) return pcg_abandon(a, it);
       double rr = 0.0;
-      spmv_true(rr);
+      if (!apply_true(rr)) return pcg_abandon(a, it);
       part[2] = rr;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       replacements++;
     }
     if (!sy.barrier()) return pcg_abandon(a, it);
     // phase B: w = A u and (w, u)
-    spmv_w(part[1]);
+    if (!apply_w(part[1])) return pcg_abandon(a, it);
     if (!sy.template reduce<3>(part, res)) return pcg_abandon(a, it);
     it++;
     const double gamma_new = res[0];
@@ -518,11 +642,11 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
       // end of an inner solve: true FP64 residual, stop or restart the recurrences from it
       if (!sy.barrier()) return pcg_abandon(a, it);
       part[0] = part[1] = part[2] = 0.0;
-      spmv_true(part[2]);
+      if (!apply_true(part[2])) return pcg_abandon(a, it);
       replacements++;
       for (int64_t i = i0; i < i1; i += is) part[0] += (double)r[i] * (double)u[i];
       if (!sy.barrier()) return pcg_abandon(a, it);
-      spmv_w(part[1]);
+      if (!apply_w(part[1])) return pcg_abandon(a, it);
       if (!sy.template reduce<3>(part, res)) return pcg_abandon(a, it);
       rho = res[2];
       if (sqrt(rho) <= atol) { converged = true; break; }
@@ -548,18 +672,18 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   }
 }
 
-template <int MODE>
+template <int MODE, int OPS>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_kernel(const __grid_constant__ PcgArgs a) {
   GridSync sy(a, blockIdx.x);
-  pcg_body<MODE>(a, blockIdx.x, sy);
+  pcg_body<MODE, OPS>(a, blockIdx.x, sy);
 }
 
 // A small system solved by one thread-block cluster (a.nblocks CTAs, the whole grid).
-template <int MODE>
+template <int MODE, int OPS>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_cluster_kernel(const __grid_constant__ PcgArgs a) {
   __shared__ double cred[8], bcast[4];
   ClusterSync sy{cluster_rank(), cluster_size(), cred, bcast, 0, 0ull, a.budget_ns, false};
-  pcg_body<MODE>(a, sy.rank, sy);
+  pcg_body<MODE, OPS>(a, sy.rank, sy);
   cluster_sync_all();            // no CTA exits while another may still read its shared memory
 }
 
@@ -574,7 +698,7 @@ struct PcgBatch {
 };
 static_assert(sizeof(PcgBatch) <= 32000, "batch arguments must fit the kernel parameter space");
 
-template <int MODE>
+template <int MODE, int OPS>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_batch_kernel(const __grid_constant__ PcgBatch b) {
   int lo = 0, hi = b.nsys - 1;              // last system whose first block is <= blockIdx.x
   while (lo < hi) {
@@ -582,7 +706,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_batch_kernel(
     if (b.start[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
   }
   GridSync sy(b.sys[lo], blockIdx.x - b.start[lo]);
-  pcg_body<MODE>(b.sys[lo], blockIdx.x - b.start[lo], sy);
+  pcg_body<MODE, OPS>(b.sys[lo], blockIdx.x - b.start[lo], sy);
 }
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -601,16 +725,32 @@ extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
   return bytes;
 }
 
-// Co-resident blocks of the cooperative kernel on the current device.
+// Co-resident blocks of the cooperative kernels on the current device: the fewest over every
+// instantiation a solve of this mode may launch (single, batched; CSR, matrix-free, both).
+// Every PCG kernel runs with PCG_WIN_BYTES of dynamic shared memory (the vector window).
+static void pcg_smem_attr(const void* f) {
+  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, PCG_WIN_BYTES);
+}
+
+static int pcg_occupancy(const void* f) {
+  int v = 0;
+  pcg_smem_attr(f);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, f, PCG_THREADS, PCG_WIN_BYTES) != cudaSuccess) v = 0;
+  return v;
+}
+
 template <int MODE>
 static int pcg_capacity() {
-  int dev = 0, sms = 0, per_sm = 0;
+  int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<MODE>, PCG_THREADS, 0);
-  int per_sm_batch = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_batch, pcg_batch_kernel<MODE>, PCG_THREADS, 0);
-  if (per_sm_batch < per_sm) per_sm = per_sm_batch;
+  int per_sm = pcg_occupancy((const void*)pcg_kernel<MODE, PCG_OPS_CSR>);
+  per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_CSR>));
+  if constexpr (MODE != NGS_PCG_REFERENCE) {
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_kernel<MODE, PCG_OPS_MF>));
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_MF>));
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_BOTH>));
+  }
   const int64_t cap = (int64_t)sms * per_sm;
   return (int)(cap < PCG_MAX_BLOCKS ? cap : PCG_MAX_BLOCKS);   // the partials area holds this many blocks
 }
@@ -636,19 +776,16 @@ extern "C" int ngs_pcg_block_capacity(int mode) {
   return capacity_of(mode);
 }
 
-// Largest cluster of pcg_cluster_kernel<MODE> the current device can run (cached per device).
-template <int MODE>
-static int pcg_cluster_limit() {
-  static int cached[64];
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && cached[dev] != 0) return cached[dev] > 0 ? cached[dev] : 0;
+// Largest cluster of pcg_cluster_kernel<MODE, *> the current device can run (cached per device): the
+// smaller of the CSR and the matrix-free instantiation.
+static int pcg_cluster_limit_of_kernel(const void* f) {
   int limit = 0;
-  if (cudaFuncSetAttribute(pcg_cluster_kernel<MODE>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
-      cudaSuccess) {
+  pcg_smem_attr(f);
+  if (cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3(PCG_CLUSTER_MAX);
     lc.blockDim = dim3(PCG_THREADS);
+    lc.dynamicSmemBytes = PCG_WIN_BYTES;
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeClusterDimension;
     attr.val.clusterDim.x = PCG_CLUSTER_MAX;
@@ -656,10 +793,21 @@ static int pcg_cluster_limit() {
     attr.val.clusterDim.z = 1;
     lc.attrs = &attr;
     lc.numAttrs = 1;
-    if (cudaOccupancyMaxPotentialClusterSize(&limit, (const void*)pcg_cluster_kernel<MODE>, &lc) != cudaSuccess)
-      limit = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&limit, f, &lc) != cudaSuccess) limit = 0;
   }
   cudaGetLastError();   // a refused query leaves no sticky error: the cooperative path is used instead
+  return limit;
+}
+
+template <int MODE>
+static int pcg_cluster_limit() {
+  static int cached[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && cached[dev] != 0) return cached[dev] > 0 ? cached[dev] : 0;
+  int limit = pcg_cluster_limit_of_kernel((const void*)pcg_cluster_kernel<MODE, PCG_OPS_CSR>);
+  if constexpr (MODE != NGS_PCG_REFERENCE)
+    limit = std::min(limit, pcg_cluster_limit_of_kernel((const void*)pcg_cluster_kernel<MODE, PCG_OPS_MF>));
   if (limit > PCG_CLUSTER_MAX) limit = PCG_CLUSTER_MAX;
   if (dev >= 0 && dev < 64) cached[dev] = limit > 0 ? limit : -1;
   return limit;
@@ -692,10 +840,11 @@ extern "C" int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode) {
   return (int)pcg_blocks_for(n, nnz, 0, capacity_of(mode));
 }
 
-static void* pcg_cluster_kernel_of(int mode) {
-  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_cluster_kernel<NGS_PCG_REFERENCE>;
-  if (mode == NGS_PCG_MIXED) return (void*)pcg_cluster_kernel<NGS_PCG_MIXED>;
-  return (void*)pcg_cluster_kernel<NGS_PCG_FP64>;
+static void* pcg_cluster_kernel_of(int mode, bool mf) {
+  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_cluster_kernel<NGS_PCG_REFERENCE, PCG_OPS_CSR>;
+  if (mode == NGS_PCG_MIXED)
+    return mf ? (void*)pcg_cluster_kernel<NGS_PCG_MIXED, PCG_OPS_MF> : (void*)pcg_cluster_kernel<NGS_PCG_MIXED, PCG_OPS_CSR>;
+  return mf ? (void*)pcg_cluster_kernel<NGS_PCG_FP64, PCG_OPS_MF> : (void*)pcg_cluster_kernel<NGS_PCG_FP64, PCG_OPS_CSR>;
 }
 
 // One cluster of `csize` CTAs solves the system (an ordinary launch: the hardware places the whole
@@ -706,7 +855,7 @@ static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3((unsigned)csize);
   lc.blockDim = dim3(PCG_THREADS);
-  lc.dynamicSmemBytes = 0;
+  lc.dynamicSmemBytes = PCG_WIN_BYTES;
   lc.stream = st;
   cudaLaunchAttribute attr;
   attr.id = cudaLaunchAttributeClusterDimension;
@@ -717,7 +866,9 @@ static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
   lc.numAttrs = 1;
   void* args[] = {&a};
   ngs_count_launch();
-  const cudaError_t e = cudaLaunchKernelExC(&lc, pcg_cluster_kernel_of(mode), args);
+  const void* f = pcg_cluster_kernel_of(mode, a.mf != 0);
+  pcg_smem_attr(f);
+  const cudaError_t e = cudaLaunchKernelExC(&lc, f, args);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }
@@ -733,14 +884,24 @@ static void pcg_clear_status(int64_t* info_dev, double* resid_dev, cudaStream_t 
 // Returns NGS_OK, an error, or 1 for an empty system (nothing to launch).  Touches no device memory.
 static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
                        int64_t* info_dev, double* resid_dev, cudaStream_t st, PcgArgs& a) {
-  if (!sys || !cfg || !info_dev || !resid_dev || sys->n < 0 || !sys->rowptr ||
-      (sys->nnz > 0 && !sys->cols && !sys->col_delta) || !sys->inv_diag)
-    return NGS_ERR_INVALID_ARG;
+  if (!sys || !cfg || !info_dev || !resid_dev || sys->n < 0 || !sys->inv_diag) return NGS_ERR_INVALID_ARG;
   const int mode = cfg->mode;
   if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64) return NGS_ERR_INVALID_ARG;
-  if (mode == NGS_PCG_REFERENCE && (!sys->vals32 || !sys->b32 || !sys->x32)) return NGS_ERR_INVALID_ARG;
-  if (mode == NGS_PCG_MIXED && (!sys->vals32 || !sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
-  if (mode == NGS_PCG_FP64 && (!sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
+  const ngs_pcg_operator* op = sys->op;
+  if (op) {
+    // matrix-free: MIXED and FP64 modes; no CSR is read
+    if (mode == NGS_PCG_REFERENCE || op->n_points < 0 || op->n_points > (int64_t)0x7fffffff || sys->nnz < 0 ||
+        (sys->n > 0 && (!op->coords || !op->stencil || !op->t_ptr || !op->grid.words)) ||
+        (op->n_points > 0 && (!op->point_rows || !op->point_phi || !op->t_point || !op->t_phi || !op->scratch64 ||
+                              (mode == NGS_PCG_MIXED && !op->scratch32))) ||
+        !sys->b64 || !sys->x64)
+      return NGS_ERR_INVALID_ARG;
+  } else {
+    if (!sys->rowptr || (sys->nnz > 0 && !sys->cols && !sys->col_delta)) return NGS_ERR_INVALID_ARG;
+    if (mode == NGS_PCG_REFERENCE && (!sys->vals32 || !sys->b32 || !sys->x32)) return NGS_ERR_INVALID_ARG;
+    if (mode == NGS_PCG_MIXED && (!sys->vals32 || !sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
+    if (mode == NGS_PCG_FP64 && (!sys->vals64 || !sys->b64 || !sys->x64)) return NGS_ERR_INVALID_ARG;
+  }
   if (!ws || ws_bytes < ngs_pcg_workspace_bytes(sys->n, mode)) return NGS_ERR_OOM;
   const int64_t n = sys->n;
   if (n == 0) return 1;
@@ -778,21 +939,43 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.wait_ns = (unsigned long long)(timeout * 1e9);
   a.budget_ns = a.wait_ns;
   a.inner_rtol = 1.0e-4;
+  a.win_cap = (int)(PCG_WIN_BYTES / pcg_vec_bytes(mode));
   const size_t mat_bytes = (size_t)sys->nnz * ((sys->col_delta ? 2 : 4) + (mode == NGS_PCG_FP64 ? 8 : 4));
   a.evict_first = mat_bytes > (size_t)96 << 20;
+  if (op) {
+    a.mf = 1;
+    a.op = *op;
+    a.rowptr = nullptr;
+    a.cols = nullptr;
+    a.cols16 = nullptr;
+    a.evict_first = 0;
+  }
   return NGS_OK;
 }
 
-static void* pcg_kernel_of(int mode) {
-  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_kernel<NGS_PCG_REFERENCE>;
-  if (mode == NGS_PCG_MIXED) return (void*)pcg_kernel<NGS_PCG_MIXED>;
-  return (void*)pcg_kernel<NGS_PCG_FP64>;
+static void* pcg_kernel_of(int mode, bool mf) {
+  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_kernel<NGS_PCG_REFERENCE, PCG_OPS_CSR>;
+  if (mode == NGS_PCG_MIXED)
+    return mf ? (void*)pcg_kernel<NGS_PCG_MIXED, PCG_OPS_MF> : (void*)pcg_kernel<NGS_PCG_MIXED, PCG_OPS_CSR>;
+  return mf ? (void*)pcg_kernel<NGS_PCG_FP64, PCG_OPS_MF> : (void*)pcg_kernel<NGS_PCG_FP64, PCG_OPS_CSR>;
 }
 
-static void* pcg_batch_kernel_of(int mode) {
-  if (mode == NGS_PCG_REFERENCE) return (void*)pcg_batch_kernel<NGS_PCG_REFERENCE>;
-  if (mode == NGS_PCG_MIXED) return (void*)pcg_batch_kernel<NGS_PCG_MIXED>;
-  return (void*)pcg_batch_kernel<NGS_PCG_FP64>;
+// ops: PCG_OPS_CSR / _MF / _BOTH, from the systems of the batch.
+template <int MODE>
+static void* pcg_batch_kernel_ops(int ops) {
+  if constexpr (MODE == NGS_PCG_REFERENCE) {
+    return (void*)pcg_batch_kernel<MODE, PCG_OPS_CSR>;
+  } else {
+    if (ops == PCG_OPS_MF) return (void*)pcg_batch_kernel<MODE, PCG_OPS_MF>;
+    if (ops == PCG_OPS_BOTH) return (void*)pcg_batch_kernel<MODE, PCG_OPS_BOTH>;
+    return (void*)pcg_batch_kernel<MODE, PCG_OPS_CSR>;
+  }
+}
+
+static void* pcg_batch_kernel_of(int mode, int ops) {
+  if (mode == NGS_PCG_REFERENCE) return pcg_batch_kernel_ops<NGS_PCG_REFERENCE>(ops);
+  if (mode == NGS_PCG_MIXED) return pcg_batch_kernel_ops<NGS_PCG_MIXED>(ops);
+  return pcg_batch_kernel_ops<NGS_PCG_FP64>(ops);
 }
 
 extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, void* ws, size_t ws_bytes,
@@ -813,8 +996,10 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   cudaMemsetAsync(a.count, 0, 8 * sizeof(unsigned int), st);
   void* args[] = {&a};
   ngs_count_launch();
-  const cudaError_t e = cudaLaunchCooperativeKernel(pcg_kernel_of(cfg->mode), dim3((unsigned)blocks),
-                                                    dim3(PCG_THREADS), args, 0, st);
+  void* f = pcg_kernel_of(cfg->mode, a.mf != 0);
+  pcg_smem_attr(f);
+  const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3((unsigned)blocks), dim3(PCG_THREADS), args, PCG_WIN_BYTES,
+                                                    st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }
@@ -873,10 +1058,13 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     pcg_clear_status(b.sys[k].info, b.sys[k].resid, st);
     cudaMemsetAsync(b.sys[k].count, 0, 8 * sizeof(unsigned int), st);
   }
+  int ops = 0;
+  for (int k = 0; k < b.nsys; k++) ops |= b.sys[k].mf ? PCG_OPS_MF : PCG_OPS_CSR;
   void* args[] = {&b};
   ngs_count_launch();
-  const cudaError_t e = cudaLaunchCooperativeKernel(pcg_batch_kernel_of(mode), dim3(total), dim3(PCG_THREADS), args,
-                                                    0, st);
+  void* f = pcg_batch_kernel_of(mode, ops);
+  pcg_smem_attr(f);
+  const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3(total), dim3(PCG_THREADS), args, PCG_WIN_BYTES, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }
@@ -913,6 +1101,7 @@ extern "C" int64_t ngs_pcg_noalloc_max_rows(void) { return kNoallocMaxRows; }
 extern "C" int ngs_pcg_solve_noalloc(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, int64_t* info_dev,
                                      double* resid_dev, ngs_stream s) {
   if (!sys || !cfg || sys->n < 0) return NGS_ERR_INVALID_ARG;
+  if (sys->op) return NGS_ERR_INVALID_ARG;                     // assembled (CSR) systems only
   if (sys->n > kNoallocMaxRows) return NGS_ERR_OOM;            // too large for the built-in scratch
   if (ngs_pcg_workspace_bytes(sys->n, cfg->mode) > kNoallocScratchBytes) return NGS_ERR_OOM;
   void* ws = nullptr;

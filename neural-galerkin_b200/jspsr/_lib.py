@@ -21,6 +21,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "buffer or workspace too small", 3:
 NGS_OK, NGS_ERR_INVALID_ARG, NGS_ERR_OOM, NGS_ERR_HASH_INSERT, NGS_ERR_NOT_CONVERGED = 0, 1, 2, 3, 4
 NGS_ERR_TOPOLOGY, NGS_ERR_CUDA, NGS_ERR_TIMEOUT = 5, 6, 7
 PCG_REFERENCE, PCG_MIXED, PCG_FP64 = 0, 1, 2
+NGS_F16, NGS_BF16, NGS_F32 = 0, 1, 2
 MAX_FIELD_LEVELS = 16
 
 vp, i32, i64, f32, f64, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_float, C.c_double, C.c_size_t
@@ -36,10 +37,17 @@ class HashTable(C.Structure):
     _fields_ = [("slots", C.c_void_p), ("nslots", C.c_int64), ("inserted", C.c_int64)]
 
 
+class PcgOperator(C.Structure):
+    """ngs_pcg_operator: the matrix-free level operator (stencil over the bitmap + point screening)."""
+    _fields_ = [("grid", Grid), ("coords", vp), ("stencil", vp), ("alpha", C.c_double), ("n_points", C.c_int64),
+                ("point_rows", vp), ("point_phi", vp), ("t_ptr", vp), ("t_point", vp), ("t_phi", vp),
+                ("scratch32", vp), ("scratch64", vp)]
+
+
 class PcgSystem(C.Structure):
     _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("rowptr", vp), ("cols", vp), ("vals32", vp),
                 ("vals64", vp), ("b32", vp), ("b64", vp), ("inv_diag", vp), ("x32", vp), ("x64", vp),
-                ("col_delta", vp)]
+                ("col_delta", vp), ("op", C.POINTER(PcgOperator))]
 
 
 class PcgConfig(C.Structure):
@@ -108,6 +116,19 @@ _SIGS = {
     "ngs_correction_screen": ([vp, vp, i64, vp, vp, f64, vp, vp], C.c_int),
     "ngs_finish_system": ([vp, i64, vp, i64, vp, vp, vp], C.c_int),
     "ngs_csr_col_delta": ([vp, vp, i64, vp, vp], C.c_int),
+    "ngs_mf_count": ([vp, i64, i64, vp, vp, vp], C.c_int),
+    "ngs_mf_fill": ([vp, vp, i64, vp, i64, vp, vp, vp, vp, vp, vp], C.c_int),
+    "ngs_mf_diag": ([vp, vp, i64, f64, f64, vp, vp], C.c_int),
+    "ngs_mf_screen_rhs": ([vp, vp, vp, i64, vp, f64, vp, vp], C.c_int),
+    "ngs_mf_apply64": ([C.POINTER(PcgOperator), i64, vp, vp, vp], C.c_int),
+    "ngs_conv_table": ([vp, vp, C.c_int, C.c_int, i64, C.c_int, vp, vp], C.c_int),
+    "ngs_conv_transpose_weight": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp], C.c_int),
+    "ngs_conv_tensor_core_ok": ([C.c_int, C.c_int, C.c_int], C.c_int),
+    "ngs_conv_gather_gemm": ([vp, i64, C.c_int, vp, i64, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp],
+                             C.c_int),
+    "ngs_conv_weight_grad_ws_bytes": ([C.c_int, C.c_int, C.c_int, i64], sz),
+    "ngs_conv_weight_grad": ([vp, i64, C.c_int, vp, i64, C.c_int, vp, vp, C.c_int, i64, C.c_int, C.c_int, vp,
+                              C.c_int, vp, sz, vp, vp], C.c_int),
     "ngs_pcg_workspace_bytes": ([i64, C.c_int], sz),
     "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
     "ngs_pcg_block_capacity": ([C.c_int], C.c_int),

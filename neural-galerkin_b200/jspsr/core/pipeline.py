@@ -109,6 +109,14 @@ class Level:
     resid: torch.Tensor = None
     col_delta: torch.Tensor = None   # int16 column - row per non-zero (when every delta fits)
     delta_ok: bool = False
+    # matrix-free operator (solver reads no CSR): the point basis transposed per row
+    mf: bool = False
+    t_ptr: torch.Tensor = None      # [n + 1] int64
+    t_point: torch.Tensor = None    # [E] int32
+    t_phi: torch.Tensor = None      # [E] float32
+    n_pairs: int = 0                # E
+    max_pairs: int = 0              # longest row list
+    stencil: torch.Tensor = None    # [125] FP64 same-level stiffness
 
 
 def _box(qmin, qmax, stride, pad=1):
@@ -308,7 +316,7 @@ class Reconstruction(DualMesher):
 
     def __init__(self, xyz: torch.Tensor, normal: torch.Tensor, voxel_size: float, depth: int = 4,
                  min_density: float = 32.0, screen_alpha: float = 4.0, screen_delta: float = 0.1,
-                 solver: str = "pcg-mixed@tol=1e-7", timings: Timings | None = None):
+                 solver: str = "pcg-mixed@tol=1e-7", timings: Timings | None = None, operator: str = "csr"):
         L.require_cuda(xyz, "xyz")
         L.require_cuda(normal, "normal")
         self.xyz = xyz.contiguous().float()
@@ -332,6 +340,14 @@ class Reconstruction(DualMesher):
         self.solve_hook = None     # callable(rec, level, d, item): hands the level's PCG to a batcher
         # largest dual-grid rank bitmap (16-byte words) before the mesh switches to sorted keys
         self.dual_grid_max_words = 1 << 27
+        # level operator of the solver: "csr" = the assembled matrix (the faster one on B200: its SpMV
+        # gathers from a shared-memory window of the vector); "matrix-free" = the stencil over the
+        # bitmap plus the point form of the screening, on the levels where the point pairs are fewer
+        # than the stiffness non-zeros (FP32-mixed and FP64 solvers)
+        if operator not in ("csr", "matrix-free"):
+            raise ValueError(f"operator must be 'csr' or 'matrix-free', not {operator!r}")
+        self.operator = operator
+        self.keep_csr = False      # also assemble the CSR of matrix-free levels (tests compare it)
 
     def _mark(self, name):
         if self.t is not None:
@@ -401,9 +417,13 @@ class Reconstruction(DualMesher):
 
     # ------------------------------------------------------------------ assembly
     def assemble(self):
-        """Splat normals, point basis, per-level CSR structure, stiffness and screening Gram."""
+        """Splat normals, point basis, and each level's operator: the CSR (stiffness + screening Gram)
+        or the matrix-free form (stencil table + the point basis transposed per row)."""
         st = L.stream()
         inv = np.float32(self.inv_vs)
+        mf_candidate = (self.operator == "matrix-free" and self.alpha > 0 and
+                        self.solver.mode in (L.PCG_MIXED, L.PCG_FP64))
+        pair_max = torch.zeros(self.depth, dtype=torch.int32, device=self.dev)
         for d, lv in enumerate(self.levels):
             if self.level_hist[d] > 0:
                 lv.normals = torch.zeros((lv.n, 3), dtype=torch.float32, device=self.dev)
@@ -418,39 +438,93 @@ class Reconstruction(DualMesher):
             L.call("ngs_stencil_count", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(counts), st)
             lv.rowptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
             L.scan(counts, out=lv.rowptr[:lv.n], total=lv.rowptr[lv.n:])
+            if mf_candidate:
+                # (point, slot) pairs per row: decides the operator, and their scan places the lists
+                pc = torch.zeros(lv.n, dtype=torch.int32, device=self.dev)
+                L.call("ngs_mf_count", L.ptr(lv.rows), self.n, lv.n, L.ptr(pc), L.ptr(pair_max[d:d + 1]), st)
+                lv.t_ptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
+                L.scan(pc, out=lv.t_ptr[:lv.n], total=lv.t_ptr[lv.n:])
         self._mark("structure")
-        # with the non-zero counts, a bound on |column - row| per level (decides the 2-byte columns)
+        # with the non-zero counts, a bound on |column - row| per level (decides the 2-byte columns), and
+        # the pair counts (decide the matrix-free operator): one synchronisation for all levels
         span = [self._row_span_bound(lv) for lv in self.levels]
-        host = torch.stack([lv.rowptr[lv.n] for lv in self.levels] + span).cpu().numpy()
-        nnz, span = host[:self.depth], host[self.depth:]
+        pairs = [lv.t_ptr[lv.n] if lv.t_ptr is not None else torch.zeros((), dtype=torch.int64, device=self.dev)
+                 for lv in self.levels]
+        host = torch.cat([torch.stack([lv.rowptr[lv.n] for lv in self.levels] + span + pairs),
+                          pair_max.long()]).cpu().numpy()
+        D = self.depth
+        nnz, span, npairs, pmax = host[:D], host[D:2 * D], host[2 * D:3 * D], host[3 * D:]
         for d, lv in enumerate(self.levels):
             lv.nnz = int(nnz[d])
-            lv.delta_ok = bool(span[d] <= 32767)
-            lv.cols = torch.empty(lv.nnz, dtype=torch.int32, device=self.dev)
-            lv.vals64 = torch.empty(lv.nnz, dtype=torch.float64, device=self.dev)
-            lv.diag_slot = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
-            st125 = L.device_table(("stencil125", lv.stride), lambda s=lv.stride: TB.stencil125(s), self.dev)
-            L.call("ngs_stencil_fill", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(lv.rowptr),
-                   L.ptr(st125), L.ptr(lv.cols), L.ptr(lv.vals64), L.ptr(lv.diag_slot), st)
-            if self.alpha > 0:
-                sf = 0.25 ** d
-                # group the points by cell: one atomic per (cell, slot) instead of per point
-                key = torch.empty(self.n, dtype=torch.int64, device=self.dev)
-                L.call("ngs_point_cell_keys", L.ptr(lv.rows), self.n, L.ptr(key), st)
-                keys, order = torch.sort(key)
-                lv.group = (keys, order)          # reused by the screening RHS terms of this level
-                L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(order),
-                       L.ptr(keys), L.ptr(lv.masks), L.ptr(lv.rowptr), sf * self.alpha, L.ptr(lv.vals64), st)
-            if lv.delta_ok:
-                # 2-byte column deltas for the solver's SpMV (6 instead of 8 bytes per non-zero)
-                lv.col_delta = torch.empty(lv.nnz, dtype=torch.int16, device=self.dev)
-                L.call("ngs_csr_col_delta", L.ptr(lv.rowptr), L.ptr(lv.cols), lv.n, L.ptr(lv.col_delta), st)
-            lv.vals32 = torch.empty(lv.nnz, dtype=torch.float32, device=self.dev)
-            lv.inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
-            L.call("ngs_finish_system", L.ptr(lv.vals64), lv.nnz, L.ptr(lv.diag_slot), lv.n, L.ptr(lv.vals32),
-                   L.ptr(lv.inv_diag), st)
+            lv.n_pairs, lv.max_pairs = int(npairs[d]), int(pmax[d])
+            # the point form costs 2 gathers per pair against one per stored non-zero; long lists
+            # (millions of points per cell on coarse levels of large scenes) stay with the Gram
+            lv.mf = bool(mf_candidate and 2 * lv.n_pairs <= lv.nnz and lv.max_pairs <= 4096)
+            lv.stencil = L.device_table(("stencil125", lv.stride), lambda s=lv.stride: TB.stencil125(s), self.dev)
+            if lv.mf:
+                self._assemble_mf(lv, d)
+            if not lv.mf or self.keep_csr:
+                self._assemble_csr(lv, d, bool(span[d] <= 32767))
         self._mark("assembly")
         return self
+
+    def _assemble_mf(self, lv: Level, d: int):
+        st = L.stream()
+        E = lv.n_pairs
+        cursor = torch.zeros(lv.n, dtype=torch.int32, device=self.dev)
+        tmp_point = torch.empty(E, dtype=torch.int32, device=self.dev)
+        tmp_phi = torch.empty(E, dtype=torch.float32, device=self.dev)
+        lv.t_point = torch.empty(E, dtype=torch.int32, device=self.dev)
+        lv.t_phi = torch.empty(E, dtype=torch.float32, device=self.dev)
+        L.call("ngs_mf_fill", L.ptr(lv.rows), L.ptr(lv.phi), self.n, L.ptr(lv.t_ptr), lv.n, L.ptr(cursor),
+               L.ptr(tmp_point), L.ptr(tmp_phi), L.ptr(lv.t_point), L.ptr(lv.t_phi), st)
+        lv.inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
+        L.call("ngs_mf_diag", L.ptr(lv.t_ptr), L.ptr(lv.t_phi), lv.n, float(TB.stencil125(lv.stride)[62]),
+               self._screen_scale(d), L.ptr(lv.inv_diag), st)
+
+    def _screen_scale(self, d: int) -> float:
+        """Screening weight of level d (reconstructor.py:122: alpha * (1/4)^d)."""
+        return 0.25 ** d * self.alpha
+
+    def _assemble_csr(self, lv: Level, d: int, delta_ok: bool):
+        st = L.stream()
+        lv.delta_ok = delta_ok
+        lv.cols = torch.empty(lv.nnz, dtype=torch.int32, device=self.dev)
+        lv.vals64 = torch.empty(lv.nnz, dtype=torch.float64, device=self.dev)
+        lv.diag_slot = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
+        L.call("ngs_stencil_fill", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(lv.rowptr),
+               L.ptr(lv.stencil), L.ptr(lv.cols), L.ptr(lv.vals64), L.ptr(lv.diag_slot), st)
+        if self.alpha > 0:
+            # group the points by cell: one atomic per (cell, slot) instead of per point
+            key = torch.empty(self.n, dtype=torch.int64, device=self.dev)
+            L.call("ngs_point_cell_keys", L.ptr(lv.rows), self.n, L.ptr(key), st)
+            keys, order = torch.sort(key)
+            lv.group = (keys, order)          # reused by the screening RHS terms of this level
+            L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(order),
+                   L.ptr(keys), L.ptr(lv.masks), L.ptr(lv.rowptr), self._screen_scale(d), L.ptr(lv.vals64), st)
+        if lv.delta_ok:
+            # 2-byte column deltas for the solver's SpMV (6 instead of 8 bytes per non-zero)
+            lv.col_delta = torch.empty(lv.nnz, dtype=torch.int16, device=self.dev)
+            L.call("ngs_csr_col_delta", L.ptr(lv.rowptr), L.ptr(lv.cols), lv.n, L.ptr(lv.col_delta), st)
+        lv.vals32 = torch.empty(lv.nnz, dtype=torch.float32, device=self.dev)
+        inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
+        L.call("ngs_finish_system", L.ptr(lv.vals64), lv.nnz, L.ptr(lv.diag_slot), lv.n, L.ptr(lv.vals32),
+               L.ptr(inv_diag), st)
+        if not lv.mf:
+            lv.inv_diag = inv_diag
+
+    def mf_operator(self, lv: Level, d: int) -> "L.PcgOperator":
+        """The C-ABI description of a matrix-free level (scratch for the per-point products included)."""
+        op = L.PcgOperator()
+        op.grid = lv.grid
+        op.coords, op.stencil, op.alpha, op.n_points = lv.coords.data_ptr(), lv.stencil.data_ptr(), \
+            self._screen_scale(d), self.n
+        op.point_rows, op.point_phi = lv.rows.data_ptr(), lv.phi.data_ptr()
+        op.t_ptr, op.t_point, op.t_phi = lv.t_ptr.data_ptr(), lv.t_point.data_ptr(), lv.t_phi.data_ptr()
+        s32 = torch.empty(self.n, dtype=torch.float32, device=self.dev)
+        s64 = torch.empty(self.n, dtype=torch.float64, device=self.dev)
+        op.scratch32, op.scratch64 = s32.data_ptr(), s64.data_ptr()
+        return op, (s32, s64)
 
     @staticmethod
     def _row_span_bound(lv: Level) -> torch.Tensor:
@@ -486,9 +560,7 @@ class Reconstruction(DualMesher):
                    lv.n, L.ptr(tc), L.ptr(tg), tc.numel(), L.ptr(rhs), st)
         sf = 0.25 ** d
         if self.alpha > 0:
-            keys, order = lv.group
-            L.call("ngs_screen_rhs_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, None, L.ptr(order),
-                   L.ptr(keys), sf * self.alpha * self.delta, L.ptr(rhs), st)
+            self._screen_rhs(lv, None, sf * self.alpha * self.delta, rhs)
         coarser = list(range(self.depth - 1, d, -1))
         if coarser:
             if self.alpha > 0:
@@ -496,9 +568,7 @@ class Reconstruction(DualMesher):
                 for dd in coarser:
                     lc = self.levels[dd]
                     L.call("ngs_point_field", L.ptr(lc.rows), L.ptr(lc.phi), self.n, L.ptr(lc.x32), L.ptr(fieldp), 1, st)
-                keys, order = lv.group
-                L.call("ngs_screen_rhs_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None, L.ptr(fieldp),
-                       L.ptr(order), L.ptr(keys), -sf * self.alpha, L.ptr(rhs), st)
+                self._screen_rhs(lv, fieldp, -sf * self.alpha, rhs)
             for dd in coarser:
                 lc = self.levels[dd]
                 tc = L.device_table(("corr_c", lv.stride, lc.stride),
@@ -510,6 +580,18 @@ class Reconstruction(DualMesher):
         lv.rhs = rhs
         return rhs
 
+    def _screen_rhs(self, lv: Level, val, scale: float, rhs: torch.Tensor):
+        """rhs += scale * sum over the level's points of phi * (val[point] or 1): by the transposed
+        pairs on a matrix-free level, by the cell-grouped points otherwise."""
+        st = L.stream()
+        if lv.mf:
+            L.call("ngs_mf_screen_rhs", L.ptr(lv.t_ptr), L.ptr(lv.t_point), L.ptr(lv.t_phi), lv.n,
+                   L.ptr(val) if val is not None else None, scale, L.ptr(rhs), st)
+        else:
+            keys, order = lv.group
+            L.call("ngs_screen_rhs_grouped", L.ptr(lv.rows), L.ptr(lv.phi), self.n, None,
+                   L.ptr(val) if val is not None else None, L.ptr(order), L.ptr(keys), scale, L.ptr(rhs), st)
+
     def pcg_item(self, lv: Level) -> "L.PcgBatchItem":
         """Output buffers, workspace and the C-ABI description of one level's PCG solve."""
         spec = self.solver
@@ -519,13 +601,23 @@ class Reconstruction(DualMesher):
         lv.resid = torch.zeros(2, dtype=torch.float64, device=self.dev)
         item = L.PcgBatchItem()
         sysd = item.sys
-        sysd.n, sysd.nnz = lv.n, lv.nnz
-        sysd.rowptr, sysd.cols, sysd.inv_diag = lv.rowptr.data_ptr(), lv.cols.data_ptr(), lv.inv_diag.data_ptr()
-        sysd.vals32, sysd.vals64 = lv.vals32.data_ptr(), lv.vals64.data_ptr()
-        b32 = lv.rhs.float()
-        sysd.b32, sysd.b64 = b32.data_ptr(), lv.rhs.data_ptr()
+        sysd.n, sysd.inv_diag = lv.n, lv.inv_diag.data_ptr()
+        keep = []
+        if lv.mf:
+            op, scratch = self.mf_operator(lv, next(d for d, l in enumerate(self.levels) if l is lv))
+            sysd.op = L.C.pointer(op)
+            sysd.nnz = 60 * lv.n + 2 * lv.n_pairs          # work of one application (block count)
+            b32 = None
+            keep += [op, scratch]
+        else:
+            sysd.nnz = lv.nnz
+            sysd.rowptr, sysd.cols = lv.rowptr.data_ptr(), lv.cols.data_ptr()
+            sysd.vals32, sysd.vals64 = lv.vals32.data_ptr(), lv.vals64.data_ptr()
+            b32 = lv.rhs.float()
+            sysd.b32 = b32.data_ptr()
+            sysd.col_delta = lv.col_delta.data_ptr() if lv.col_delta is not None else None
+        sysd.b64 = lv.rhs.data_ptr()
         sysd.x32, sysd.x64 = lv.x32.data_ptr(), lv.x64.data_ptr()
-        sysd.col_delta = lv.col_delta.data_ptr() if lv.col_delta is not None else None
         cfg = item.cfg
         cfg.mode, cfg.max_iter, cfg.tol = spec.mode, spec.maxiter, spec.tol
         cfg.res_fix, cfg.replace_every, cfg.blocks, cfg.timeout_s = int(spec.res_fix), spec.replace, 0, spec.timeout
@@ -533,7 +625,7 @@ class Reconstruction(DualMesher):
         ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.dev)
         item.ws, item.ws_bytes = ws.data_ptr(), ws_bytes
         item.info_dev, item.resid_dev = lv.info.data_ptr(), lv.resid.data_ptr()
-        lv._keep = (ws, b32)
+        lv._keep = (ws, b32, *keep)
         return item
 
     def _solve_level(self, lv: Level, d: int = 0):
