@@ -276,12 +276,124 @@ def dual_marching_cubes_indices(dual_centers_hash_data: HashLookupData, expand_p
     return [acc, cnt]
 
 
+# ----------------------------------------------------------------------------- sparse convolution
+_CONV_DTYPES = {torch.float16: L.NGS_F16, torch.bfloat16: L.NGS_BF16, torch.float32: L.NGS_F32}
+
+
+def _conv_dtype(t: torch.Tensor) -> int:
+    if t.dtype not in _CONV_DTYPES:
+        raise TypeError(f"sparse convolution takes float16, bfloat16 or float32 features, not {t.dtype}")
+    return _CONV_DTYPES[t.dtype]
+
+
+def _offset_starts(neighbor_offset, K: int, device):
+    """int64 [K+1] exclusive prefix of the per-offset pair counts, on the device, and the largest count."""
+    sizes = torch.as_tensor(neighbor_offset).reshape(-1).to(device="cpu", dtype=torch.int64)
+    if sizes.numel() != K:
+        raise ValueError(f"neighbor_offset has {sizes.numel()} entries for a kernel of {K} offsets")
+    starts = torch.zeros(K + 1, dtype=torch.int64)
+    starts[1:] = torch.cumsum(sizes, 0)
+    return starts.to(device), int(sizes.max()) if K else 0
+
+
+def _conv_table(neighbor_map, starts, K, key_col, n_rows, mid):
+    table = torch.empty((n_rows, K), dtype=torch.int32, device=neighbor_map.device)
+    L.call("ngs_conv_table", L.ptr(neighbor_map), L.ptr(starts), K, key_col, n_rows, mid, L.ptr(table), L.stream())
+    return table
+
+
+def _gather_gemm(x, table, bt, ncols, out):
+    err = torch.zeros(1, dtype=torch.int32, device=x.device)
+    dt = _conv_dtype(x)
+    out_f32 = int(out.dtype == torch.float32)
+    L.call("ngs_conv_gather_gemm", L.ptr(x), x.shape[0], x.shape[1], L.ptr(table), table.shape[0], table.shape[1],
+           L.ptr(bt), ncols, dt, L.ptr(out), out_f32, L.ptr(err), L.stream())
+    return err
+
+
+def _raise_device_error(err):
+    code = int(err.item())
+    if code:
+        raise L.NgsError(code, "sparse convolution")
+
+
+def convolution_forward_cuda(in_feat, out_feat, kernel, neighbor_map, neighbor_offset, transpose: bool,
+                             no_acc: bool):
+    """``sparse_op.convolution_forward_cuda`` (convolution_cuda.cu:52-174): out_feat [M, Cout] receives
+    sum over offsets k and pairs (i, o) of offset k of in_feat[i] @ kernel[k] (pairs (map[:,0], map[:,1]),
+    read the other way round when ``transpose``).  As in the reference, when the kernel volume is odd,
+    the input and output counts agree and ``no_acc`` is false, the centre offset is the identity over
+    all rows and out_feat is overwritten; otherwise the sum is added to out_feat.  One fused gather-GEMM
+    kernel on the tensor cores (16-bit features, FP32 accumulation)."""
+    _check_cuda(in_feat, out_feat, kernel, neighbor_map)
+    if in_feat.shape[1] != kernel.shape[1]:
+        raise ValueError("Input feature size and kernel size mismatch")
+    K, cin, cout = kernel.shape
+    x = in_feat.contiguous()
+    w = kernel.contiguous().to(x.dtype)
+    nbmap = neighbor_map.int().contiguous()
+    starts, _ = _offset_starts(neighbor_offset, K, x.device)
+    n_out = out_feat.shape[0]
+    precompute_mid = K % 2 == 1 and x.shape[0] == n_out and not no_acc
+    key_col = 0 if transpose else 1
+    table = _conv_table(nbmap, starts, K, key_col, n_out, K // 2 if precompute_mid else -1)
+    wt = torch.empty((K, cout, cin), dtype=w.dtype, device=w.device)
+    L.call("ngs_conv_transpose_weight", L.ptr(w), K, cin, cout, _conv_dtype(w), L.ptr(wt), L.stream())
+    if precompute_mid and out_feat.is_contiguous() and out_feat.dtype == x.dtype:
+        err = _gather_gemm(x, table, wt, cout, out_feat)
+    else:
+        res = torch.empty((n_out, cout), dtype=out_feat.dtype, device=x.device)
+        err = _gather_gemm(x, table, wt, cout, res)
+        if precompute_mid:
+            out_feat.copy_(res)
+        else:
+            out_feat.add_(res)
+    _raise_device_error(err)
+
+
+def convolution_backward_cuda(in_feat, grad_in_feat, grad_out_feat, kernel, grad_kernel, neighbor_map,
+                              neighbor_offset, transpose: bool):
+    """``sparse_op.convolution_backward_cuda`` (convolution_cuda.cu:176-282): grad_in_feat = sum over pairs
+    (i, o) of offset k of grad_out[o] @ kernel[k]^T (gathered per input row, no scatter) and
+    grad_kernel[k] = sum over the pairs of in_feat[i]^T grad_out[o] (a GEMM over the pairs, split over
+    CTAs and reduced in a fixed order); both are overwritten, as the reference zeroes them."""
+    _check_cuda(in_feat, grad_in_feat, grad_out_feat, kernel, grad_kernel, neighbor_map)
+    K, cin, cout = kernel.shape
+    x = in_feat.contiguous()
+    gy = grad_out_feat.contiguous().to(x.dtype)
+    w = kernel.contiguous().to(x.dtype)
+    nbmap = neighbor_map.int().contiguous()
+    starts, max_pairs = _offset_starts(neighbor_offset, K, x.device)
+    in_col = 1 if transpose else 0
+    table = _conv_table(nbmap, starts, K, in_col, x.shape[0], -1)
+    grad_in_feat.resize_(x.shape)
+    grad_kernel.resize_(kernel.shape)
+    gi = grad_in_feat if (grad_in_feat.is_contiguous() and grad_in_feat.dtype == x.dtype) else \
+        torch.empty(x.shape, dtype=x.dtype, device=x.device)
+    err = _gather_gemm(gy, table, w, cin, gi)
+    if gi is not grad_in_feat:
+        grad_in_feat.copy_(gi)
+    dt = _conv_dtype(x)
+    gk = grad_kernel if (grad_kernel.is_contiguous() and grad_kernel.dtype == x.dtype) else \
+        torch.empty(kernel.shape, dtype=x.dtype, device=x.device)
+    ws_bytes = L.load().ngs_conv_weight_grad_ws_bytes(K, cin, cout, max_pairs)
+    ws = torch.empty(max(ws_bytes, 16), dtype=torch.uint8, device=x.device)
+    L.call("ngs_conv_weight_grad", L.ptr(x), x.shape[0], cin, L.ptr(gy), gy.shape[0], cout, L.ptr(nbmap), L.ptr(starts),
+           K, max_pairs, in_col, dt, L.ptr(gk), int(gk.dtype == torch.float32), L.ptr(ws), ws.numel(), L.ptr(err),
+           L.stream())
+    if gk is not grad_kernel:
+        grad_kernel.copy_(gk)
+    _raise_device_error(err)
+
+
 # ----------------------------------------------------------------------------- module namespaces
 common = _common = SimpleNamespace(hash_cuda=hash_cuda, kernel_hash_cuda=kernel_hash_cuda,
                                    build_hash_table=build_hash_table, hash_table_query=hash_table_query,
                                    HashLookupData=HashLookupData)
 sparse_op = _sparse_op = SimpleNamespace(sparse_meshgrid=sparse_meshgrid, screened_multiplication=screened_multiplication,
-                                         screened_multiplication_backward=screened_multiplication_backward)
+                                         screened_multiplication_backward=screened_multiplication_backward,
+                                         convolution_forward_cuda=convolution_forward_cuda,
+                                         convolution_backward_cuda=convolution_backward_cuda)
 integration = _integration = SimpleNamespace(ddi_forward=ddi_forward, ddi_backward=ddi_backward)
 sparse_solve = _sparse_solve = SimpleNamespace(solve_pcg_diag=solve_pcg_diag, solve_cusparse=solve_cusparse,
                                                init_cusolver=init_cusolver)
