@@ -402,6 +402,12 @@ int ngs_mf_diag(const int64_t* t_ptr, const float* t_phi, int64_t V, double sten
 int ngs_mf_screen_rhs(const int64_t* t_ptr, const int32_t* t_point, const float* t_phi, int64_t V, const float* val,
                       double scale, double* rhs, ngs_stream s);
 int ngs_mf_apply64(const ngs_pcg_operator* op, int64_t n, const double* x, double* y, ngs_stream s);
+/* The screening Gram scale * sum_p phi_p phi_p^T added into an assembled stencil CSR (rowptr, the
+ * 128-bit offset masks of ngs_stencil_count, vals FP64) from the transposed pairs; no atomics, fixed
+ * summation order (ref: csrc/sparse_op/sparse_product.cu:100-137 + jspsr/core/reconstructor.py:181-185). */
+int ngs_mf_gram(const int64_t* t_ptr, const int32_t* t_point, const float* t_phi, int64_t V, const int32_t* point_rows,
+                const float* point_phi, const uint32_t* masks, const int64_t* rowptr, double scale, double* vals,
+                ngs_stream s);
 
 /* ======================================================================= sparse convolution
  * ref: csrc/sparse_op/convolution_cuda.cu:52-174 (convolution_forward_cuda), :176-282

@@ -10,18 +10,6 @@
 // reference's second hash table keyed by (row, col) pairs.
 #include "ngs_common.cuh"
 
-NGS_DEV int popc_below(const uint4 m, int o) {
-  // number of set bits of the 128-bit mask m strictly below bit o
-  const unsigned w[4] = {m.x, m.y, m.z, m.w};
-  int c = 0;
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int lo = i * 32;
-    if (o >= lo + 32) c += __popc(w[i]);
-    else if (o > lo) c += __popc(w[i] & ((1u << (o - lo)) - 1u));
-  }
-  return c;
-}
 
 // ----------------------------------------------------------------------------- structure
 // One warp per row: lane l < 25 owns the stencil column (dx, dy) = (l / 5 - 2, l % 5 - 2) and its

@@ -51,17 +51,18 @@ __global__ void mf_scatter_kernel(const int32_t* __restrict__ rows, const float*
   }
 }
 
-// ... then each row's pairs ranked by point index (a point occurs at most once per row): one warp per
-// row, every lane counts the smaller indices of its entries.  The order, and with it every sum over
-// the pairs, is then independent of the atomic arrival order.
+// ... then each row's pairs ranked by point index (a point occurs at most once per row): eight lanes
+// per row (rows hold ~7 pairs on a fine level), every lane counts the smaller indices of its entries.
+// The order, and with it every sum over the pairs, is then independent of the atomic arrival order.
 __global__ void mf_rank_kernel(const int64_t* __restrict__ t_ptr, int64_t V, const int32_t* __restrict__ tmp_point,
                                const float* __restrict__ tmp_phi, int32_t* __restrict__ t_point,
                                float* __restrict__ t_phi) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = ngs_gstride() >> 5;
-  for (int64_t row = ngs_gtid() >> 5; row < V; row += warps) {
+  constexpr int G = 8;
+  const int sub = threadIdx.x & (G - 1);
+  const int64_t groups = ngs_gstride() / G;
+  for (int64_t row = ngs_gtid() / G; row < V; row += groups) {
     const int64_t e0 = t_ptr[row], len = t_ptr[row + 1] - e0;
-    for (int64_t j = lane; j < len; j += 32) {
+    for (int64_t j = sub; j < len; j += G) {
       const int32_t pj = tmp_point[e0 + j];
       int64_t rank = 0;
       for (int64_t k = 0; k < len; k++) rank += tmp_point[e0 + k] < pj;
@@ -84,7 +85,7 @@ extern "C" int ngs_mf_fill(const int32_t* point_rows, const float* point_phi, in
                                                                                 t_ptr, cursor, tmp_point, tmp_phi);
   NGS_CHECK_LAUNCH();
   ngs_count_launch();
-  mf_rank_kernel<<<ngs_blocks(V * 32, 256), 256, 0, (cudaStream_t)s>>>(t_ptr, V, tmp_point, tmp_phi, t_point, t_phi);
+  mf_rank_kernel<<<ngs_blocks(V * 8, 256), 256, 0, (cudaStream_t)s>>>(t_ptr, V, tmp_point, tmp_phi, t_point, t_phi);
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }
@@ -162,6 +163,80 @@ extern "C" int ngs_mf_apply64(const ngs_pcg_operator* op, int64_t n, const doubl
   }
   ngs_count_launch();
   mf_rows64_kernel<<<ngs_blocks(n, 256), 256, 0, st>>>(*op, n, x, y);
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
+// ----------------------------------------------------------------------------- screening Gram
+// The level's screening Gram alpha * sum_p phi_p phi_p^T added into the assembled CSR (ref: the pair
+// products of csrc/sparse_op/sparse_product.cu:100-137 summed into the LHS at
+// jspsr/core/reconstructor.py:181-185), from the transposed pairs: row i owns its slots, so one warp
+// per row adds, for each point p among the row's pairs (in pair order), phi_p(i) * phi_p(j) for the
+// point's 27 rows j -- lanes 0..26 hold the point's rows and values; within one point the 27 rows sit
+// at 27 distinct stencil offsets from i, so the per-offset sums of the row (shared memory) take no
+// atomics, and the order of the sums is fixed.  One add per present slot at the end.
+constexpr int MF_GRAM_THREADS = 256;
+
+__global__ void __launch_bounds__(MF_GRAM_THREADS) mf_gram_kernel(
+    const int64_t* __restrict__ t_ptr, const int32_t* __restrict__ t_point, const float* __restrict__ t_phi,
+    int64_t V, const int32_t* __restrict__ prow, const float* __restrict__ pphi, const uint4* __restrict__ masks,
+    const int64_t* __restrict__ rowptr, double scale, double* __restrict__ vals) {
+  __shared__ double acc[MF_GRAM_THREADS / 32][125];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t warps = ngs_gstride() >> 5;
+  const int ax = lane / 9, ay = (lane / 3) % 3, az = lane % 3;
+  for (int64_t i = ngs_gtid() >> 5; i < V; i += warps) {
+    for (int o = lane; o < 125; o += 32) acc[w][o] = 0.0;
+    __syncwarp();
+    const int64_t e0 = t_ptr[i], e1 = t_ptr[i + 1];
+    // the row's pairs 32 at a time on the lanes, then two points per step with both points' rows and
+    // values in flight together
+    for (int64_t base = e0; base < e1; base += 32) {
+      const int cnt = (int)min((int64_t)32, e1 - base);
+      const int32_t my_p = lane < cnt ? t_point[base + lane] : 0;
+      const float my_f = lane < cnt ? t_phi[base + lane] : 0.f;
+      for (int q = 0; q < cnt; q += 2) {
+        const bool two = q + 1 < cnt;
+        const int64_t pa = __shfl_sync(0xffffffffu, my_p, q), pb = __shfl_sync(0xffffffffu, my_p, two ? q + 1 : q);
+        const double fa = (double)__shfl_sync(0xffffffffu, my_f, q);
+        const double fb = (double)__shfl_sync(0xffffffffu, my_f, two ? q + 1 : q);
+        const int32_t ra = lane < 27 ? __ldg(prow + pa * 27 + lane) : -1;
+        const float va = lane < 27 ? __ldg(pphi + pa * 27 + lane) : 0.f;
+        const int32_t rb = (lane < 27 && two) ? __ldg(prow + pb * 27 + lane) : -1;
+        const float vb = (lane < 27 && two) ? __ldg(pphi + pb * 27 + lane) : 0.f;
+        const int aa = __ffs((int)__ballot_sync(0xffffffffu, ra == (int32_t)i)) - 1;
+        const int ab = __ffs((int)__ballot_sync(0xffffffffu, rb == (int32_t)i)) - 1;
+        if (ra >= 0 && aa >= 0) {
+          const int o = (ax - aa / 9 + 2) * 25 + (ay - (aa / 3) % 3 + 2) * 5 + (az - aa % 3 + 2);
+          acc[w][o] += fa * (double)va;
+        }
+        __syncwarp();
+        if (rb >= 0 && ab >= 0) {
+          const int o = (ax - ab / 9 + 2) * 25 + (ay - (ab / 3) % 3 + 2) * 5 + (az - ab % 3 + 2);
+          acc[w][o] += fb * (double)vb;
+        }
+        __syncwarp();
+      }
+    }
+    const uint4 m = masks[i];
+    const int64_t base = rowptr[i];
+    for (int o = lane; o < 125; o += 32) {
+      const unsigned word = o < 32 ? m.x : o < 64 ? m.y : o < 96 ? m.z : m.w;
+      if ((word >> (o & 31)) & 1u) vals[base + popc_below(m, o)] += scale * acc[w][o];
+    }
+    __syncwarp();
+  }
+}
+
+extern "C" int ngs_mf_gram(const int64_t* t_ptr, const int32_t* t_point, const float* t_phi, int64_t V,
+                           const int32_t* point_rows, const float* point_phi, const uint32_t* masks,
+                           const int64_t* rowptr, double scale, double* vals, ngs_stream s) {
+  if (V < 0 || (V > 0 && (!t_ptr || !t_point || !t_phi || !point_rows || !point_phi || !masks || !rowptr || !vals)))
+    return NGS_ERR_INVALID_ARG;
+  if (V == 0) return NGS_OK;
+  ngs_count_launch();
+  mf_gram_kernel<<<ngs_blocks(V * 32, MF_GRAM_THREADS), MF_GRAM_THREADS, 0, (cudaStream_t)s>>>(
+      t_ptr, t_point, t_phi, V, point_rows, point_phi, reinterpret_cast<const uint4*>(masks), rowptr, scale, vals);
   NGS_CHECK_LAUNCH();
   return NGS_OK;
 }

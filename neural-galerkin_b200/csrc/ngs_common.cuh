@@ -74,6 +74,20 @@ NGS_DEV int64_t grid_word_index(const ngs_grid& g, int x, int y, int z, int* bit
   return ((int64_t)i * g.dims[1] + j) * g.zwords + (k >> 6);
 }
 
+// A row's slot of stencil offset o (0..124) under its 128-bit offset mask: the set bits below o.
+NGS_DEV int popc_below(const uint4 m, int o) {
+  // number of set bits of the 128-bit mask m strictly below bit o
+  const unsigned w[4] = {m.x, m.y, m.z, m.w};
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int lo = i * 32;
+    if (o >= lo + 32) c += __popc(w[i]);
+    else if (o > lo) c += __popc(w[i] & ((1u << (o - lo)) - 1u));
+  }
+  return c;
+}
+
 // ----------------------------------------------------------------------------- B-spline
 // Quadratic B-spline scaled by 2 (jspsr/bases/bezier_tensor.py:17-22,36-54).
 NGS_DEV float bspline(float x) {

@@ -121,6 +121,7 @@ _SIGS = {
     "ngs_mf_diag": ([vp, vp, i64, f64, f64, vp, vp], C.c_int),
     "ngs_mf_screen_rhs": ([vp, vp, vp, i64, vp, f64, vp, vp], C.c_int),
     "ngs_mf_apply64": ([C.POINTER(PcgOperator), i64, vp, vp, vp], C.c_int),
+    "ngs_mf_gram": ([vp, vp, vp, i64, vp, vp, vp, vp, f64, vp, vp], C.c_int),
     "ngs_conv_table": ([vp, vp, C.c_int, C.c_int, i64, C.c_int, vp, vp], C.c_int),
     "ngs_conv_transpose_weight": ([vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp], C.c_int),
     "ngs_conv_tensor_core_ok": ([C.c_int, C.c_int, C.c_int], C.c_int),

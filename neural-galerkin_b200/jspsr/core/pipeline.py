@@ -100,7 +100,6 @@ class Level:
     nnz: int = 0
     rows: torch.Tensor = None      # point basis [N, 27]
     phi: torch.Tensor = None
-    group: tuple = None            # (sorted cell keys, point order) of the screening terms
     normals: torch.Tensor = None   # splatted normal data (points with this exact level)
     rhs: torch.Tensor = None
     x64: torch.Tensor = None
@@ -110,6 +109,8 @@ class Level:
     col_delta: torch.Tensor = None   # int16 column - row per non-zero (when every delta fits)
     delta_ok: bool = False
     # matrix-free operator (solver reads no CSR): the point basis transposed per row
+    group: tuple = None            # (sorted cell keys, point order): screening terms of long-pair levels
+    pair_form: bool = False        # screening terms gathered per row from the transposed pairs
     mf: bool = False
     t_ptr: torch.Tensor = None      # [n + 1] int64
     t_point: torch.Tensor = None    # [E] int32
@@ -348,6 +349,10 @@ class Reconstruction(DualMesher):
             raise ValueError(f"operator must be 'csr' or 'matrix-free', not {operator!r}")
         self.operator = operator
         self.keep_csr = False      # also assemble the CSR of matrix-free levels (tests compare it)
+        # longest pair list of a level whose screening terms go by rows from the transposed pairs (no
+        # atomics, no sort); 0: every CSR level groups its points by cell (sort + FP64 atomics per cell
+        # chunk), which measured faster on the 300k benchmark (33.5 against 35.0 ms per reconstruction)
+        self.pair_row_limit = 0
 
     def _mark(self, name):
         if self.t is not None:
@@ -438,8 +443,9 @@ class Reconstruction(DualMesher):
             L.call("ngs_stencil_count", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(counts), st)
             lv.rowptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
             L.scan(counts, out=lv.rowptr[:lv.n], total=lv.rowptr[lv.n:])
-            if mf_candidate:
-                # (point, slot) pairs per row: decides the operator, and their scan places the lists
+            if self.alpha > 0 and (mf_candidate or self.pair_row_limit > 0):
+                # (point, slot) pairs per row (the screening terms in gather form; their counts also
+                # decide the matrix-free operator), the scan places the lists
                 pc = torch.zeros(lv.n, dtype=torch.int32, device=self.dev)
                 L.call("ngs_mf_count", L.ptr(lv.rows), self.n, lv.n, L.ptr(pc), L.ptr(pair_max[d:d + 1]), st)
                 lv.t_ptr = torch.empty(lv.n + 1, dtype=torch.int64, device=self.dev)
@@ -461,6 +467,13 @@ class Reconstruction(DualMesher):
             # (millions of points per cell on coarse levels of large scenes) stay with the Gram
             lv.mf = bool(mf_candidate and 2 * lv.n_pairs <= lv.nnz and lv.max_pairs <= 4096)
             lv.stencil = L.device_table(("stencil125", lv.stride), lambda s=lv.stride: TB.stencil125(s), self.dev)
+            # screening terms per row from the pairs, unless some row has so many (coarse levels of large
+            # scenes: millions of points in one cell) that a row's serial walk would dominate -- those
+            # levels group the points by cell instead (one sort, FP64 atomics per cell chunk)
+            lv.pair_form = bool(self.alpha > 0 and lv.t_ptr is not None and
+                                (lv.max_pairs <= self.pair_row_limit or lv.mf))
+            if lv.pair_form:
+                self._fill_pairs(lv)
             if lv.mf:
                 self._assemble_mf(lv, d)
             if not lv.mf or self.keep_csr:
@@ -468,7 +481,8 @@ class Reconstruction(DualMesher):
         self._mark("assembly")
         return self
 
-    def _assemble_mf(self, lv: Level, d: int):
+    def _fill_pairs(self, lv: Level):
+        """The point basis transposed per row: for every row, its (point, phi) pairs in point order."""
         st = L.stream()
         E = lv.n_pairs
         cursor = torch.zeros(lv.n, dtype=torch.int32, device=self.dev)
@@ -478,6 +492,9 @@ class Reconstruction(DualMesher):
         lv.t_phi = torch.empty(E, dtype=torch.float32, device=self.dev)
         L.call("ngs_mf_fill", L.ptr(lv.rows), L.ptr(lv.phi), self.n, L.ptr(lv.t_ptr), lv.n, L.ptr(cursor),
                L.ptr(tmp_point), L.ptr(tmp_phi), L.ptr(lv.t_point), L.ptr(lv.t_phi), st)
+
+    def _assemble_mf(self, lv: Level, d: int):
+        st = L.stream()
         lv.inv_diag = torch.empty(lv.n, dtype=torch.float32, device=self.dev)
         L.call("ngs_mf_diag", L.ptr(lv.t_ptr), L.ptr(lv.t_phi), lv.n, float(TB.stencil125(lv.stride)[62]),
                self._screen_scale(d), L.ptr(lv.inv_diag), st)
@@ -494,8 +511,12 @@ class Reconstruction(DualMesher):
         lv.diag_slot = torch.empty(lv.n, dtype=torch.int64, device=self.dev)
         L.call("ngs_stencil_fill", lv.grid, L.ptr(lv.coords), lv.n, L.ptr(lv.masks), L.ptr(lv.rowptr),
                L.ptr(lv.stencil), L.ptr(lv.cols), L.ptr(lv.vals64), L.ptr(lv.diag_slot), st)
-        if self.alpha > 0:
-            # group the points by cell: one atomic per (cell, slot) instead of per point
+        if self.alpha > 0 and lv.pair_form:
+            # the screening Gram by rows from the transposed pairs: no atomics, fixed summation order
+            L.call("ngs_mf_gram", L.ptr(lv.t_ptr), L.ptr(lv.t_point), L.ptr(lv.t_phi), lv.n, L.ptr(lv.rows),
+                   L.ptr(lv.phi), L.ptr(lv.masks), L.ptr(lv.rowptr), self._screen_scale(d), L.ptr(lv.vals64), st)
+        elif self.alpha > 0:
+            # group the points by cell: one FP64 atomic per (cell chunk, slot) instead of per point
             key = torch.empty(self.n, dtype=torch.int64, device=self.dev)
             L.call("ngs_point_cell_keys", L.ptr(lv.rows), self.n, L.ptr(key), st)
             keys, order = torch.sort(key)
@@ -581,10 +602,10 @@ class Reconstruction(DualMesher):
         return rhs
 
     def _screen_rhs(self, lv: Level, val, scale: float, rhs: torch.Tensor):
-        """rhs += scale * sum over the level's points of phi * (val[point] or 1): by the transposed
-        pairs on a matrix-free level, by the cell-grouped points otherwise."""
+        """rhs += scale * sum over the level's points of phi * (val[point] or 1): gathered per row from the
+        transposed pairs (no atomics), or through the cell-grouped points on long-pair levels."""
         st = L.stream()
-        if lv.mf:
+        if lv.pair_form:
             L.call("ngs_mf_screen_rhs", L.ptr(lv.t_ptr), L.ptr(lv.t_point), L.ptr(lv.t_phi), lv.n,
                    L.ptr(val) if val is not None else None, scale, L.ptr(rhs), st)
         else:

@@ -117,7 +117,9 @@ def test_diagonal_and_screening_rhs_equal_csr_path(recs, name):
                L.ptr(inv), st)
         inv_csr = (1.0 / lv.vals64[lv.diag_slot]).float()
         assert rel(inv, inv_csr) <= 1e-7, (name, d)
-        keys, order = lv.group
+        cell = torch.empty(rec.n, dtype=torch.int64, device=DEV)
+        L.call("ngs_point_cell_keys", L.ptr(lv.rows), rec.n, L.ptr(cell), st)
+        keys, order = torch.sort(cell)
         field = torch.rand(rec.n, device=DEV)
         for f in (None, field):
             a = torch.zeros(lv.n, dtype=torch.float64, device=DEV)

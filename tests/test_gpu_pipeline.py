@@ -35,6 +35,25 @@ def cases(golden):
     return out
 
 
+def pairs_of(rec, lv):
+    """The level's point basis transposed per row, built through the C ABI."""
+    from jspsr import _lib as L
+    st = L.stream()
+    counts = torch.zeros(lv.n, dtype=torch.int32, device=lv.rows.device)
+    mx = torch.zeros(1, dtype=torch.int32, device=lv.rows.device)
+    L.call("ngs_mf_count", L.ptr(lv.rows), rec.n, lv.n, L.ptr(counts), L.ptr(mx), st)
+    t_ptr = torch.empty(lv.n + 1, dtype=torch.int64, device=lv.rows.device)
+    L.scan(counts, out=t_ptr[:lv.n], total=t_ptr[lv.n:])
+    E = int(t_ptr[lv.n])
+    cursor = torch.zeros(lv.n, dtype=torch.int32, device=lv.rows.device)
+    tmp = (torch.empty(E, dtype=torch.int32, device=lv.rows.device), torch.empty(E, device=lv.rows.device))
+    t_point = torch.empty(E, dtype=torch.int32, device=lv.rows.device)
+    t_phi = torch.empty(E, device=lv.rows.device)
+    L.call("ngs_mf_fill", L.ptr(lv.rows), L.ptr(lv.phi), rec.n, L.ptr(t_ptr), lv.n, L.ptr(cursor), L.ptr(tmp[0]),
+           L.ptr(tmp[1]), L.ptr(t_point), L.ptr(t_phi), st)
+    return t_ptr, t_point, t_phi
+
+
 def run_gpu(g, solver="pcg-mixed@tol=1e-9"):
     from jspsr.core.pipeline import Reconstruction
     vs, depth, md, alpha = g["params"]
@@ -134,7 +153,7 @@ def test_grouped_screening_terms(gpu_runs, name):
         keys = torch.empty_like(ref)
         L.call("ngs_point_cell_keys", L.ptr(lv.rows), rec.n, L.ptr(keys), L.stream())
         assert torch.equal(keys, ref)
-        skeys, order = lv.group
+        skeys, order = torch.sort(keys)
         field = torch.rand(rec.n, device=lv.rows.device)
         for f in (None, field):
             a = torch.zeros(lv.n, dtype=torch.float64, device=lv.rows.device)
@@ -148,6 +167,51 @@ def test_grouped_screening_terms(gpu_runs, name):
                    L.ptr(f) if f is not None else None, L.ptr(order), L.ptr(skeys), 0.75 if f is None else -0.75,
                    L.ptr(b), L.stream())
             assert rel(b.cpu().numpy(), a.cpu().numpy()) < 1e-12
+            t_ptr, t_point, t_phi = pairs_of(rec, lv)   # the pair form: gathered per row
+            c = torch.zeros_like(a)
+            L.call("ngs_mf_screen_rhs", L.ptr(t_ptr), L.ptr(t_point), L.ptr(t_phi), lv.n,
+                   L.ptr(f) if f is not None else None, 0.75 if f is None else -0.75, L.ptr(c), L.stream())
+            assert rel(c.cpu().numpy(), a.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gram_from_pairs_equals_cell_grouped_atomics(gpu_runs, name):
+    """The production screening Gram (per row from the transposed pairs, no atomics) equals the
+    cell-grouped Gram with FP64 atomics up to FP64 summation order, on the assembled pattern."""
+    from jspsr import _lib as L
+    rec = gpu_runs[name][0]
+    for d, lv in enumerate(rec.levels):
+        st = L.stream()
+        t_ptr, t_point, t_phi = pairs_of(rec, lv)
+        a = torch.zeros(lv.nnz, dtype=torch.float64, device=lv.rows.device)
+        b = torch.zeros_like(a)
+        L.call("ngs_mf_gram", L.ptr(t_ptr), L.ptr(t_point), L.ptr(t_phi), lv.n, L.ptr(lv.rows),
+               L.ptr(lv.phi), L.ptr(lv.masks), L.ptr(lv.rowptr), 1.5, L.ptr(a), st)
+        keys = torch.empty(rec.n, dtype=torch.int64, device=lv.rows.device)
+        L.call("ngs_point_cell_keys", L.ptr(lv.rows), rec.n, L.ptr(keys), st)
+        skeys, order = torch.sort(keys)
+        L.call("ngs_screen_gram_grouped", L.ptr(lv.rows), L.ptr(lv.phi), rec.n, None, L.ptr(order), L.ptr(skeys),
+               L.ptr(lv.masks), L.ptr(lv.rowptr), 1.5, L.ptr(b), st)
+        assert float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) < 1e-13, d
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_pair_form_reconstruction_equals_cell_grouping(cases, gpu_runs, name):
+    """The whole reconstruction with every level's screening terms in pair form (the Gram per row
+    from the transposed pairs, no atomics, no sort) solves the same systems."""
+    from jspsr.core.pipeline import Reconstruction
+    g, _, _ = cases[name]
+    vs, depth, md, alpha = g["params"]
+    rec = Reconstruction(torch.from_numpy(g["xyz"]).cuda(), torch.from_numpy(g["nrm"]).cuda(), vs, int(depth), md,
+                         alpha, solver="pcg-mixed@tol=1e-9")
+    rec.pair_row_limit = 1 << 30
+    rec.run()
+    rec.check_solves()
+    assert all(lv.pair_form for lv in rec.levels)
+    for lv, ref in zip(rec.levels, gpu_runs[name][0].levels):
+        assert rel(lv.vals64.cpu().numpy(), ref.vals64.cpu().numpy()) < 1e-13
+        assert rel(lv.rhs.cpu().numpy(), ref.rhs.cpu().numpy()) < 1e-6      # coarse solutions enter at tol
+        assert rel(lv.x64.cpu().numpy(), ref.x64.cpu().numpy()) < TOL
 
 
 @pytest.mark.parametrize("name", CASES)
