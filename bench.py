@@ -278,6 +278,10 @@ def conv_leg(cin=64, cout=64, reps=10):
 
     fwd = timed(lambda: ext.sparse_op.convolution_forward_cuda(x, out, w, nbmaps, nbsizes, False, False))
     bwd = timed(lambda: ext.sparse_op.convolution_backward_cuda(x, gx, gy, w, gw, nbmaps, nbsizes, False))
+    # the input-gradient kernel alone (the rest of the backward pass is the weight gradient)
+    starts_dev, _ = ext._offset_starts(nbsizes, 27, x.device)
+    table_in = ext._conv_table(nbmaps, starts_dev, 27, 0, n, -1)
+    dgrad = timed(lambda: ext._gather_gemm(gy, table_in, w, cin, gx))
     starts = np.concatenate([[0], np.cumsum(nbsizes.numpy())])
 
     def reference_forward():
@@ -291,7 +295,8 @@ def conv_leg(cin=64, cout=64, reps=10):
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("bf16_tflops", 1590.0)
     return {"voxels": n, "pairs": pairs, "cin": cin, "cout": cout, "dtype": "bf16 in, fp32 accumulate",
-            "forward_ms": fwd, "backward_ms": bwd, "forward_tflops": flops / fwd / 1e9,
+            "forward_ms": fwd, "backward_ms": bwd, "input_grad_kernel_ms": dgrad,
+            "weight_grad_ms": bwd - dgrad, "forward_tflops": flops / fwd / 1e9,
             "backward_tflops": 2 * flops / bwd / 1e9, "peak_bf16_tflops": peak,
             "forward_frac_of_peak": flops / fwd / 1e9 / peak,
             "reference_algorithm_torch_forward_ms": ref_fwd, "forward_speedup_vs_reference_algorithm": ref_fwd / fwd,

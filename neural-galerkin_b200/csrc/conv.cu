@@ -80,12 +80,24 @@ NGS_DEV uint64_t kmajor_sw128_desc(uint32_t saddr) {
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
+// Shared-memory matrix descriptor of an MN-major tile with 128-byte swizzle: each 128-byte row holds 64
+// consecutive M (or N) elements at one K index, 8 K rows form a 1024-byte swizzle atom (stride byte
+// offset 1024 between the atoms along K), and the 64-element atoms along M sit 8 KB apart (leading
+// byte offset: 64 K rows per stage).  A K step of 16 advances the start address by two atoms.
+constexpr uint32_t MN_ATOM_BYTES = 64 * 128;
+NGS_DEV uint64_t mnmajor_sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(MN_ATOM_BYTES >> 4) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
 // Instruction descriptor of kind::f16 with FP32 accumulation, both operands K-major.
 // bf16: 1 = BF16 inputs, 0 = FP16 inputs (A and B always share the type).
 NGS_DEV uint32_t f16_idesc(int m, int n, int bf16) {
   const uint32_t fmt = bf16 ? 1u : 0u;
   return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
+// The same with both operands MN-major (bits 15 and 16).
+NGS_DEV uint32_t f16_idesc_mn(int m, int n, int bf16) { return f16_idesc(m, n, bf16) | (1u << 15) | (1u << 16); }
 
 NGS_DEV void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
   asm volatile(
@@ -188,7 +200,8 @@ struct TileShape {
 constexpr uint32_t A_BYTES = BM * 128;   // 16 KB
 
 template <typename Fill, typename Store>
-NGS_DEV void run_tile(const TileShape& t, uint8_t* smem, Fill& fill, Store& store, int bf16, int* error) {
+NGS_DEV void run_tile(const TileShape& t, uint8_t* smem, Fill& fill, Store& store, int bf16, int* error,
+                      bool mn_major = false) {
   __shared__ uint64_t full_bar[8], empty_bar[8], done_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
@@ -223,7 +236,7 @@ NGS_DEV void run_tile(const TileShape& t, uint8_t* smem, Fill& fill, Store& stor
     }
   } else if (lane == 0) {
     // one thread issues the MMAs of every stage, then commits the stage back to the producers
-    const uint32_t idesc = f16_idesc(BM, t.n, bf16);
+    const uint32_t idesc = mn_major ? f16_idesc_mn(BM, t.n, bf16) : f16_idesc(BM, t.n, bf16);
     for (int s = 0; s < t.steps; s++) {
       const int st = s % S;
       if (!mbar_wait(&full_bar[st], (uint32_t)(s / S) & 1u, &abort_flag)) break;
@@ -231,7 +244,9 @@ NGS_DEV void run_tile(const TileShape& t, uint8_t* smem, Fill& fill, Store& stor
       const uint32_t a = smem_u32(smem + (size_t)st * t.stage_bytes), b = a + A_BYTES;
       const int ks = ksteps_of[st];
       for (int kk = 0; kk < ks; kk++)
-        umma_f16(tmem, kmajor_sw128_desc(a + kk * 32), kmajor_sw128_desc(b + kk * 32), idesc,
+        umma_f16(tmem,
+                 mn_major ? mnmajor_sw128_desc(a + kk * 2048) : kmajor_sw128_desc(a + kk * 32),
+                 mn_major ? mnmajor_sw128_desc(b + kk * 2048) : kmajor_sw128_desc(b + kk * 32), idesc,
                  (s > 0 || kk > 0) ? 1u : 0u);
       umma_commit(&empty_bar[st]);
     }
@@ -387,6 +402,7 @@ struct WeightGrad {
   int splits;
   int m_tiles;               // ceil(cin / 128)
   float* part;               // [K, splits, cin, cout]
+  int mn;                    // channels in multiples of 64: rows copied as they are into MN-major stages
   int bf16;
   int stages;
   uint32_t stage_bytes;
@@ -435,6 +451,32 @@ __global__ void __launch_bounds__(conv::THREADS, 1) conv_wgrad_kernel(const __gr
     }
     return (int)min((int64_t)BK, p_count - pc);
   };
+  // MN-major form: the stage's K index is the pair, each 128-byte row 64 consecutive channels of one
+  // pair, so a producer copies 16-byte pieces of its pair's rows as they are (no transposition)
+  auto fill_mn = [&](int s, uint8_t* a, uint8_t* b, int p) -> int {
+    const int64_t pc = (c_begin + s) * BK;
+    const int kk = p & 63, q = p >> 6;
+    const int64_t pair = pc + kk;
+    int32_t xi = -1, yo = -1;
+    if (pair < p_count) {
+      xi = __ldg(g.nbmaps + 2 * (p_begin + pair) + g.in_col);
+      yo = __ldg(g.nbmaps + 2 * (p_begin + pair) + 1 - g.in_col);
+    }
+    const bool hx = xi >= 0 && xi < g.n_in, hy = yo >= 0 && yo < g.n_out;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {                    // A: 16 chunks of 8 channels, 4 per quarter
+      const int c = q * 4 + j, ch = m0 + c * 8;
+      const uint4 v = (hx && ch < g.cin) ? ldg16(g.x + (int64_t)xi * g.cin + ch) : make_uint4(0, 0, 0, 0);
+      *reinterpret_cast<uint4*>(a + (c >> 3) * MN_ATOM_BYTES + sw128(kk, c & 7)) = v;
+    }
+    const int per = N / 32;                          // B: N / 8 chunks, a quarter each
+    for (int j = 0; j < per; j++) {
+      const int c = q * per + j, ch = n0 + c * 8;
+      const uint4 v = hy ? ldg16(g.gy + (int64_t)yo * g.cout + ch) : make_uint4(0, 0, 0, 0);
+      *reinterpret_cast<uint4*>(b + (c >> 3) * MN_ATOM_BYTES + sw128(kk, c & 7)) = v;
+    }
+    return (int)min((int64_t)BK, p_count - pc);
+  };
   float* part = g.part + ((int64_t)k * g.splits + split) * g.cin * g.cout;
   auto store = [&](int row, int col, const float (&v)[16]) {
     if (m0 + row < g.cin) {
@@ -443,7 +485,8 @@ __global__ void __launch_bounds__(conv::THREADS, 1) conv_wgrad_kernel(const __gr
       for (int j = 0; j < 4; j++) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     }
   };
-  run_tile(t, smem, fill, store, g.bf16, g.error);
+  if (g.mn) run_tile(t, smem, fill_mn, store, g.bf16, g.error, true);
+  else run_tile(t, smem, fill, store, g.bf16, g.error);
 }
 
 // grad_w[k, c, n] = sum over splits (in order) of part[k, split, c, n]; FP32 or 16-bit out.
@@ -660,6 +703,7 @@ extern "C" int ngs_conv_weight_grad(const void* x, int64_t n_in, int cin, const 
   g.splits = (int)(need / ((size_t)K * cin * cout * sizeof(float)));
   g.m_tiles = (cin + conv::BM - 1) / conv::BM;
   g.part = static_cast<float*>(ws);
+  g.mn = cin % 64 == 0 && cout % 64 == 0 && aligned16(x) && aligned16(gy);
   g.bf16 = dtype == NGS_BF16;
   g.error = error_dev;
   size_t smem = 0;

@@ -121,13 +121,17 @@ def test_strided_kernel_between_two_sets():
     assert rel(out, ref) <= 1e-5
 
 
-@pytest.mark.parametrize("dtype", [torch.bfloat16, torch.float32])
-def test_backward_matches_autograd_of_reference_loop(dtype):
+@pytest.mark.parametrize("dtype,cin,cout", [(torch.bfloat16, 64, 48), (torch.float32, 64, 48),
+                                            (torch.bfloat16, 64, 64), (torch.float16, 128, 256),
+                                            (torch.bfloat16, 192, 64)])
+def test_backward_matches_autograd_of_reference_loop(dtype, cin, cout):
+    """Channels in multiples of 64 take the weight gradient's MN-major stages (pair rows copied as
+    they are), others the transposing K-major stages; FP32 the CUDA cores."""
     from jspsr.sparse_conv import ConvolutionFunction
     n, nbmaps, nbsizes = voxel_maps(seed=4)
     gen = torch.Generator(device="cpu").manual_seed(11)
-    x = torch.randn(n, 64, generator=gen).to(DEV, dtype).requires_grad_(True)
-    w = (torch.randn(27, 64, 48, generator=gen) / 8).to(DEV, dtype).requires_grad_(True)
+    x = torch.randn(n, cin, generator=gen).to(DEV, dtype).requires_grad_(True)
+    w = (torch.randn(27, cin, cout, generator=gen) / cin ** 0.5).to(DEV, dtype).requires_grad_(True)
     y = ConvolutionFunction.apply(x, w, nbmaps, nbsizes, (n, n), False, False)
     g = torch.randn(y.shape, generator=gen).to(DEV, dtype)
     gx, gw = torch.autograd.grad(y, (x, w), g)
