@@ -147,50 +147,77 @@ NGS_DEV T ld_mat(const T* p) {
   else return __ldg(p);
 }
 
-// y = A v over rows [row0, row1): eight lanes per row.  epi(row, acc, pre(row)) consumes each
-// row's product (lane 0 of its group) and returns a contribution to the thread's partial sum.
-// The gathered vector is read with plain loads: it was written earlier in this launch.  Ends with a
-// block barrier, after which every thread may read the rows written by the epilogue.
+// One round of a row's entries for lane sub: entries j0, j0 + L, ...; entries past the row's end
+// gather the row's own element (the diagonal's, cached) and weigh it by zero, so that the gathers
+// need no predicate.
+template <bool STREAM, bool DELTA, int L, int U, typename MT>
+NGS_DEV void spmv_load_round(const PcgArgs& a, const MT* __restrict__ vals, int64_t row, int64_t j0, int64_t e1,
+                             int32_t (&c)[U], MT (&m)[U]) {
+#pragma unroll
+  for (int k = 0; k < U; k++) {
+    const int64_t j = j0 + (int64_t)k * L;
+    if constexpr (DELTA) c[k] = (int32_t)row + (j < e1 ? (int32_t)ld_mat<STREAM>(a.cols16 + j) : 0);
+    else c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : (int32_t)row;
+    m[k] = j < e1 ? ld_mat<STREAM>(vals + j) : (MT)0;
+  }
+}
+
+// The round's products summed in the matrix type (two chains), returned in ACC: one conversion per
+// round instead of two per product; the FP64 refinement of the mixed mode works from the true
+// residual, so this rounding only shapes the inner iterations.
+template <typename MT, typename VT, typename ACC, int U>
+NGS_DEV ACC spmv_round_sum(const VT* v, int64_t voff, const int32_t (&c)[U], const MT (&m)[U]) {
+  VT xv[U];
+#pragma unroll
+  for (int k = 0; k < U; k++) xv[k] = v[c[k] - voff];
+  MT r0 = (MT)0, r1 = (MT)0;
+#pragma unroll
+  for (int k = 0; k < U; k += 2) {
+    r0 += m[k] * (MT)xv[k];
+    r1 += m[k + 1] * (MT)xv[k + 1];
+  }
+  return (ACC)r0 + (ACC)r1;
+}
+
+// y = A v over rows [row0, row1): eight lanes per row, a warp on four consecutive rows (their entries
+// are contiguous: coalesced matrix loads).  epi(row, acc, pre(row)) consumes each row's product (lane
+// 0 of its group) and returns a contribution to the thread's partial sum.  The gathered vector is
+// read with plain loads: it was written earlier in this launch.  Software-pipelined over the group's
+// rows: the next row's pointers and first round of entries are loaded before this row's gathers are
+// consumed (a row otherwise waits on three dependent round trips: row pointer, matrix entries,
+// gathered vector).  Rounds of four entries per lane keep the loop at 64 registers (two 512-thread
+// blocks per SM); the prefetch is unconditional -- past the group's last row it reads an empty
+// range -- so that the arrays stay in registers.  Ends with a block barrier, after which every
+// thread may read the rows written by the epilogue.
 template <bool STREAM, bool DELTA, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
 NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
                          int64_t row1, Pre pre, Epi epi, double& dsum) {
   constexpr int L = PCG_ROW_LANES;
+  constexpr int U = 4;
   const int sub = threadIdx.x & (L - 1);
   const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
   const int64_t step = blockDim.x / L;
-  for (int64_t row = row0 + threadIdx.x / L; row < row1; row += step) {
-    const int64_t e0 = a.rowptr[row], e1 = a.rowptr[row + 1];
+  int64_t row = row0 + threadIdx.x / L;
+  int64_t e0 = 0, e1 = 0;
+  if (row < row1) {
+    e0 = a.rowptr[row];
+    e1 = a.rowptr[row + 1];
+  }
+  int32_t c[U];
+  MT m[U];
+  spmv_load_round<STREAM, DELTA, L, U>(a, vals, row, e0 + sub, e1, c, m);
+  for (; row < row1; row += step) {
+    const int64_t ce0 = e0, ce1 = e1, nrow = row + step;
+    const bool more = nrow < row1;
+    e0 = more ? a.rowptr[nrow] : 0;
+    e1 = more ? a.rowptr[nrow + 1] : 0;
     const double2 ax = pre(row);
-    ACC acc = (ACC)0;
-    // rounds of U entries per lane, predicated: a 5x5x5 stencil row (<= 125 entries, ~60 on a
-    // surface) takes one or two rounds, with all of a round's loads and gathers in flight
-    constexpr int U = 8;
-    for (int64_t j0 = e0 + sub; j0 < e1; j0 += U * L) {
-      int32_t c[U];
-      MT m[U];
-      // entries past the row's end gather the row's own element (cached: the diagonal's) and weigh
-      // it by zero, so that the gathers need no predicate
-#pragma unroll
-      for (int k = 0; k < U; k++) {
-        const int64_t j = j0 + (int64_t)k * L;
-        if constexpr (DELTA) c[k] = (int32_t)row + (j < e1 ? (int32_t)ld_mat<STREAM>(a.cols16 + j) : 0);
-        else c[k] = j < e1 ? ld_mat<STREAM>(a.cols + j) : (int32_t)row;
-        m[k] = j < e1 ? ld_mat<STREAM>(vals + j) : (MT)0;
-      }
-      VT xv[U];
-#pragma unroll
-      for (int k = 0; k < U; k++) xv[k] = v[c[k] - voff];
-      // the round's products summed in the matrix type (two chains), the round sum accumulated in ACC:
-      // one conversion per round instead of two per product; the FP64 refinement of the mixed mode
-      // works from the true residual, so this rounding only shapes the inner iterations
-      MT r0 = (MT)0, r1 = (MT)0;
-#pragma unroll
-      for (int k = 0; k < U; k += 2) {
-        r0 += m[k] * (MT)xv[k];
-        r1 += m[k + 1] * (MT)xv[k + 1];
-      }
-      acc += (ACC)r0 + (ACC)r1;
+    ACC acc = spmv_round_sum<MT, VT, ACC, U>(v, voff, c, m);
+    for (int64_t j0 = ce0 + sub + U * L; j0 < ce1; j0 += U * L) {     // the row's further rounds
+      spmv_load_round<STREAM, DELTA, L, U>(a, vals, row, j0, ce1, c, m);
+      acc += spmv_round_sum<MT, VT, ACC, U>(v, voff, c, m);
     }
+    spmv_load_round<STREAM, DELTA, L, U>(a, vals, more ? nrow : row, e0 + sub, e1, c, m);
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
     if (sub == 0) dsum += epi(row, (double)acc, ax);
