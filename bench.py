@@ -525,14 +525,21 @@ def main():
         plain_rec, _, _ = step(solver=PLAIN_SOLVER, profile=True)
         plain_solve = plain_rec.pcg_ms
         plain_iters = {d: int(lv.info[0]) for d, lv in enumerate(plain_rec.levels)}
+        plain_rec = None                 # each comparator's hierarchy is released once read (large scenes)
         step(solver=FP64_SOLVER)         # warm-up of the FP64 kernel, as above
         fp64_rec, _, _ = step(solver=FP64_SOLVER, profile=True)
         fp64_solve = fp64_rec.pcg_ms
+        fp64_iters = {d: int(lv.info[0]) for d, lv in enumerate(fp64_rec.levels)}
+        fp64_rec = None
+        torch.cuda.empty_cache()
         # the matrix-free operator (stencil over the bitmap + point form of the screening) on the
         # levels where it applies, same solver
         step(operator="matrix-free")
         mf_rec, _, _ = step(profile=True, operator="matrix-free")
         mf_solve = mf_rec.pcg_ms
+        mf_levels = [d for d, lv in enumerate(mf_rec.levels) if lv.mf]
+        mf_rec = None
+        torch.cuda.empty_cache()
         # errors against every level solved to 1e-12 in FP64 on the GPU: field at the input points,
         # solutions, and mesh vertices matched by their primal-sample pair
         ref64, v64, f64 = step(solver=EXACT_SOLVER)
@@ -557,7 +564,7 @@ def main():
                  "solve_ms": {"mixed": mixed_solve, "plain_fp64_host_driven": sum(plain_solve.values()),
                               "fp64_persistent_same_tol": sum(fp64_solve.values()),
                               "mixed_matrix_free_operator": sum(mf_solve.values())},
-                 "matrix_free_levels": [d for d, lv in enumerate(mf_rec.levels) if lv.mf],
+                 "matrix_free_levels": mf_levels,
                  "matrix_free_pcg_ms_per_level": mf_solve,
                  "solve_speedup_vs_plain_fp64": sum(plain_solve.values()) / mixed_solve,
                  "solve_speedup_vs_fp64_persistent": sum(fp64_solve.values()) / mixed_solve,
@@ -567,7 +574,7 @@ def main():
                                          "sample_sign_flips": flips},
                  "pcg_ms_per_level": pcg_ms, "pcg_iters_per_level": {d: s["iters"] for d, s in stats.items()},
                  "plain_fp64_iters_per_level": plain_iters,
-                 "fp64_same_tol_iters_per_level": {d: int(lv.info[0]) for d, lv in enumerate(fp64_rec.levels)},
+                 "fp64_same_tol_iters_per_level": fp64_iters,
                  "mesh": {"vertices": int(v.shape[0]), "faces": int(f.shape[0])}}
 
     # ---------------------------------------------------------------- learned-basis and serving legs
