@@ -320,6 +320,12 @@ typedef struct ngs_pcg_system {
   const int16_t* col_delta;  /* [nnz] optional: column - row of every entry; when given the solver
                                 reads these 2-byte deltas instead of the 4-byte columns (NULL: cols) */
   const ngs_pcg_operator* op;/* optional: matrix-free operator instead of the CSR (NULL: CSR) */
+  int64_t band;              /* optional: a bound on |column - row| over the matrix, for a CSR whose
+                                columns increase within every row (0: unknown, or unsorted rows).
+                                When a block's rows plus 2 band fit the solver's shared-memory
+                                window, each block stages its slice of the search vector there;
+                                otherwise the launch reserves no shared memory for it and the space
+                                stays with the L1 cache that the gathers hit */
 } ngs_pcg_system;
 
 typedef struct ngs_pcg_config {

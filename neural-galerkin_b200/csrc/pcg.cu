@@ -182,16 +182,17 @@ NGS_DEV ACC spmv_round_sum(const VT* v, int64_t voff, const int32_t (&c)[U], con
 // y = A v over rows [row0, row1): eight lanes per row, a warp on four consecutive rows (their entries
 // are contiguous: coalesced matrix loads).  epi(row, acc, pre(row)) consumes each row's product (lane
 // 0 of its group) and returns a contribution to the thread's partial sum.  The gathered vector is
-// read with plain loads: it was written earlier in this launch.  Software-pipelined over the group's
-// rows: the next row's pointers and first round of entries are loaded before this row's gathers are
-// consumed (a row otherwise waits on three dependent round trips: row pointer, matrix entries,
-// gathered vector).  Rounds of four entries per lane keep the loop at 64 registers (two 512-thread
-// blocks per SM); the prefetch is unconditional -- past the group's last row it reads an empty
-// range -- so that the arrays stay in registers.  Ends with a block barrier, after which every
-// thread may read the rows written by the epilogue.
+// read with plain loads: it was written earlier in this launch.  Both forms end with a block barrier,
+// after which every thread may read the rows written by the epilogue.
+//
+// Software-pipelined form (2-byte column deltas): the next row's pointers and first round of entries
+// are loaded before this row's gathers are consumed (a row otherwise waits on three dependent round
+// trips: row pointer, matrix entries, gathered vector).  Rounds of four entries per lane keep the
+// loop at 64 registers (two 512-thread blocks per SM); the prefetch is unconditional -- past the
+// group's last row it reads an empty range -- so that the arrays stay in registers.
 template <bool STREAM, bool DELTA, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
-NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
-                         int64_t row1, Pre pre, Epi epi, double& dsum) {
+NGS_DEV void spmv_rows_piped(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
+                             int64_t row1, Pre pre, Epi epi, double& dsum) {
   constexpr int L = PCG_ROW_LANES;
   constexpr int U = 4;
   const int sub = threadIdx.x & (L - 1);
@@ -225,6 +226,36 @@ NGS_DEV void spmv_rows_t(const PcgArgs& a, const MT* __restrict__ vals, const VT
   // the epilogue wrote rows that other threads of the block read next (their rows in phase A)
   __syncthreads();
 }
+
+// Row-at-a-time form (4-byte columns): rounds of eight entries per lane, all of a round's loads and
+// gathers in flight; a 5x5x5 stencil row (<= 125 entries, ~60 on a surface) takes one or two
+// rounds.  With 4-byte columns this form is the faster one on large matrices (the level 0 of a
+// 5M-point room: 94 against 98 ms), with 2-byte deltas the pipelined one (the level 0 of a
+// 300k-point cloud: 9.3 against 9.7 ms).
+template <bool STREAM, bool DELTA, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
+NGS_DEV void spmv_rows_plain(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
+                             int64_t row1, Pre pre, Epi epi, double& dsum) {
+  constexpr int L = PCG_ROW_LANES;
+  constexpr int U = 8;
+  const int sub = threadIdx.x & (L - 1);
+  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+  const int64_t step = blockDim.x / L;
+  for (int64_t row = row0 + threadIdx.x / L; row < row1; row += step) {
+    const int64_t e0 = a.rowptr[row], e1 = a.rowptr[row + 1];
+    const double2 ax = pre(row);
+    ACC acc = (ACC)0;
+    for (int64_t j0 = e0 + sub; j0 < e1; j0 += U * L) {
+      int32_t c[U];
+      MT m[U];
+      spmv_load_round<STREAM, DELTA, L, U>(a, vals, row, j0, e1, c, m);
+      acc += spmv_round_sum<MT, VT, ACC, U>(v, voff, c, m);
+    }
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(gmask, acc, o);
+    if (sub == 0) dsum += epi(row, (double)acc, ax);
+  }
+  __syncthreads();
+}
 // The streaming choice is a template argument: one load form per instantiation (a runtime choice
 // per load cost 7 % of the level-0 solve and forced register spills).
 template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
@@ -232,11 +263,11 @@ NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* 
                        int64_t row1, Pre pre, Epi epi, double& dsum) {
   // the column encoding too: 2-byte deltas when the caller supplied them, 4-byte columns otherwise
   if (a.cols16) {
-    if (a.evict_first) spmv_rows_t<true, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
-    else spmv_rows_t<false, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+    if (a.evict_first) spmv_rows_piped<true, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+    else spmv_rows_piped<false, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
   } else {
-    if (a.evict_first) spmv_rows_t<true, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
-    else spmv_rows_t<false, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+    if (a.evict_first) spmv_rows_plain<true, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+    else spmv_rows_plain<false, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
   }
 }
 
@@ -754,7 +785,8 @@ extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
 
 // Co-resident blocks of the cooperative kernels on the current device: the fewest over every
 // instantiation a solve of this mode may launch (single, batched; CSR, matrix-free, both).
-// Every PCG kernel runs with PCG_WIN_BYTES of dynamic shared memory (the vector window).
+// A PCG kernel runs with PCG_WIN_BYTES of dynamic shared memory (the vector window) or none; the
+// occupancy queries assume the window, so that the capacity holds for either launch.
 static void pcg_smem_attr(const void* f) {
   cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, PCG_WIN_BYTES);
 }
@@ -874,6 +906,20 @@ static void* pcg_cluster_kernel_of(int mode, bool mf) {
   return mf ? (void*)pcg_cluster_kernel<NGS_PCG_FP64, PCG_OPS_MF> : (void*)pcg_cluster_kernel<NGS_PCG_FP64, PCG_OPS_CSR>;
 }
 
+// Whether the blocks of a system stage their slice of the search vector in shared memory (the
+// window): only when the caller bounded the bandwidth and every block's column range fits, rows per
+// block + 2 band.  A launch whose systems take no window reserves no shared memory for it, so that
+// the space stays with the L1 cache the gathers hit: a window reserved for blocks that cannot use it
+// cost 7 % of the level-0 solve of a 300k-point cloud (half of its blocks do not fit) and 9 % on a
+// 5M-point room.
+static void pcg_set_window(PcgArgs& a, int mode, int64_t band, int64_t nblocks) {
+  const int64_t cap = PCG_WIN_BYTES / (int64_t)pcg_vec_bytes(mode);
+  const int64_t rows = nblocks > 0 ? (a.n + nblocks - 1) / nblocks : a.n;
+  a.win_cap = (!a.mf && band > 0 && rows + 2 * band <= cap) ? (int)cap : 0;
+}
+
+static size_t pcg_win_smem(const PcgArgs& a) { return a.win_cap > 0 ? PCG_WIN_BYTES : 0; }
+
 // One cluster of `csize` CTAs solves the system (an ordinary launch: the hardware places the whole
 // cluster at once, so the cluster barrier needs no cooperative launch).
 static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
@@ -882,7 +928,7 @@ static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3((unsigned)csize);
   lc.blockDim = dim3(PCG_THREADS);
-  lc.dynamicSmemBytes = PCG_WIN_BYTES;
+  lc.dynamicSmemBytes = pcg_win_smem(a);
   lc.stream = st;
   cudaLaunchAttribute attr;
   attr.id = cudaLaunchAttributeClusterDimension;
@@ -966,7 +1012,7 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   a.wait_ns = (unsigned long long)(timeout * 1e9);
   a.budget_ns = a.wait_ns;
   a.inner_rtol = 1.0e-4;
-  a.win_cap = (int)(PCG_WIN_BYTES / pcg_vec_bytes(mode));
+  a.win_cap = 0;                       // decided with the block count (pcg_set_window)
   const size_t mat_bytes = (size_t)sys->nnz * ((sys->col_delta ? 2 : 4) + (mode == NGS_PCG_FP64 ? 8 : 4));
   a.evict_first = mat_bytes > (size_t)96 << 20;
   if (op) {
@@ -1014,18 +1060,22 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   pcg_clear_status(info_dev, resid_dev, st);
   if (rc == 1) return NGS_OK;
   const int csize = pcg_cluster_for(a.n, a.nnz, cfg->blocks, cluster_limit_of(cfg->mode));
-  if (csize > 0) return launch_cluster(a, cfg->mode, csize, st);
+  if (csize > 0) {
+    pcg_set_window(a, cfg->mode, sys->band, csize);
+    return launch_cluster(a, cfg->mode, csize, st);
+  }
   const int cap = capacity_of(cfg->mode);
   if (cap < 1) return NGS_ERR_CUDA;
   const int64_t blocks = pcg_blocks_for(a.n, a.nnz, cfg->blocks, cap);
   if (blocks < 1) return NGS_ERR_INVALID_ARG;
   a.nblocks = (unsigned int)blocks;
+  pcg_set_window(a, cfg->mode, sys->band, blocks);
   cudaMemsetAsync(a.count, 0, 8 * sizeof(unsigned int), st);
   void* args[] = {&a};
   ngs_count_launch();
   void* f = pcg_kernel_of(cfg->mode, a.mf != 0);
   pcg_smem_attr(f);
-  const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3((unsigned)blocks), dim3(PCG_THREADS), args, PCG_WIN_BYTES,
+  const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3((unsigned)blocks), dim3(PCG_THREADS), args, pcg_win_smem(a),
                                                     st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
@@ -1061,6 +1111,7 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     if (rc != NGS_OK) return rc;
     const int csize = pcg_cluster_for(a.n, a.nnz, it.cfg.blocks, climit);
     if (csize > 0) {                         // solved by its own cluster, as it would be alone
+      pcg_set_window(a, mode, it.sys.band, csize);
       small[nsmall] = a;
       small_size[nsmall++] = csize;
       continue;
@@ -1069,6 +1120,7 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     if (blocks < 1) return NGS_ERR_INVALID_ARG;
     if (total + blocks > (unsigned)cap) return NGS_ERR_INVALID_ARG;   // not co-resident: split the batch
     a.nblocks = (unsigned int)blocks;
+    pcg_set_window(a, mode, it.sys.band, blocks);       // as it would be alone: the same bits
     b.start[b.nsys] = total;
     b.sys[b.nsys++] = a;
     total += (unsigned)blocks;
@@ -1086,12 +1138,16 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
     cudaMemsetAsync(b.sys[k].count, 0, 8 * sizeof(unsigned int), st);
   }
   int ops = 0;
-  for (int k = 0; k < b.nsys; k++) ops |= b.sys[k].mf ? PCG_OPS_MF : PCG_OPS_CSR;
+  size_t smem = 0;
+  for (int k = 0; k < b.nsys; k++) {
+    ops |= b.sys[k].mf ? PCG_OPS_MF : PCG_OPS_CSR;
+    smem = std::max(smem, pcg_win_smem(b.sys[k]));
+  }
   void* args[] = {&b};
   ngs_count_launch();
   void* f = pcg_batch_kernel_of(mode, ops);
   pcg_smem_attr(f);
-  const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3(total), dim3(PCG_THREADS), args, PCG_WIN_BYTES, st);
+  const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3(total), dim3(PCG_THREADS), args, smem, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
 }

@@ -47,7 +47,7 @@ class PcgOperator(C.Structure):
 class PcgSystem(C.Structure):
     _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("rowptr", vp), ("cols", vp), ("vals32", vp),
                 ("vals64", vp), ("b32", vp), ("b64", vp), ("inv_diag", vp), ("x32", vp), ("x64", vp),
-                ("col_delta", vp), ("op", C.POINTER(PcgOperator))]
+                ("col_delta", vp), ("op", C.POINTER(PcgOperator)), ("band", C.c_int64)]
 
 
 class PcgConfig(C.Structure):

@@ -32,6 +32,7 @@ below), and the normal data through the divergence integrals.
 from __future__ import annotations
 
 from dataclasses import dataclass, field
+from types import SimpleNamespace
 from typing import Dict, List, Optional
 
 import numpy as np
@@ -40,7 +41,7 @@ import torch
 from .. import _lib as L
 from ..bases import tables as TB
 from ._hash_backend import VoxelLevel
-from .pipeline import parse_solver
+from .pipeline import Reconstruction, parse_solver
 
 
 # ----------------------------------------------------------------------------- geometry of one level
@@ -58,6 +59,7 @@ class LevelGeometry:
     slot_row: torch.Tensor = None     # int64 [nnz]: row of every CSR slot
     slot_rel: torch.Tensor = None     # float [nnz, 3]: column centre - row centre, in voxels
     nnz: int = 0
+    band: int = 0                     # bound on |column - row| (the solver's shared-memory window)
     pt_rows: torch.Tensor = None      # int32 [N, 27]: the basis functions touching each screening point
     pt_local: torch.Tensor = None     # float [N, 27, 3]: the point relative to each of their centres, voxels
     group: tuple = None               # (cell keys sorted, point order): the Gram's point grouping
@@ -73,7 +75,13 @@ def _stencil(geo: LevelGeometry):
     L.call("ngs_stencil_count", geo.level.grid, L.ptr(geo.level.coords), n, L.ptr(geo.masks), L.ptr(counts), st)
     geo.rowptr = torch.empty(n + 1, dtype=torch.int64, device=dev)
     L.scan(counts, out=geo.rowptr[:n], total=geo.rowptr[n:])
-    geo.nnz = int(geo.rowptr[n].item())
+    # the non-zero count and a bound on |column - row| from the rank bitmap: one synchronisation
+    if n > 0:
+        lvb = SimpleNamespace(grid=geo.level.grid, words=geo.level.words, n=n)
+        host = torch.stack([geo.rowptr[n], Reconstruction._row_span_bound(lvb)]).cpu()
+        geo.nnz, geo.band = int(host[0]), int(host[1])
+    else:
+        geo.nnz, geo.band = 0, 0
     geo.cols = torch.empty(geo.nnz, dtype=torch.int32, device=dev)
     scratch = torch.empty(geo.nnz, dtype=torch.float64, device=dev)
     geo.diag_slot = torch.empty(n, dtype=torch.int64, device=dev)
@@ -231,6 +239,7 @@ def solve_levels(jobs, spec):
         s.rowptr, s.cols, s.inv_diag = geo.rowptr.data_ptr(), geo.cols.data_ptr(), sysm.inv_diag.data_ptr()
         s.vals32, s.vals64 = sysm.vals32.data_ptr(), sysm.vals64.data_ptr()
         s.b32, s.b64, s.x32, s.x64 = b32.data_ptr(), b.data_ptr(), x32.data_ptr(), x64.data_ptr()
+        s.band = geo.band
         c = it.cfg
         c.mode, c.max_iter, c.tol, c.res_fix = mode, spec.maxiter, spec.tol, int(spec.res_fix)
         c.replace_every, c.blocks, c.timeout_s = spec.replace, 0, spec.timeout

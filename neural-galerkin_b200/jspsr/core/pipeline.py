@@ -108,6 +108,7 @@ class Level:
     resid: torch.Tensor = None
     col_delta: torch.Tensor = None   # int16 column - row per non-zero (when every delta fits)
     delta_ok: bool = False
+    band: int = 0                    # bound on |column - row| (decides the solver's shared-memory window)
     # matrix-free operator (solver reads no CSR): the point basis transposed per row
     group: tuple = None            # (sorted cell keys, point order): screening terms of long-pair levels
     pair_form: bool = False        # screening terms gathered per row from the transposed pairs
@@ -462,6 +463,7 @@ class Reconstruction(DualMesher):
         nnz, span, npairs, pmax = host[:D], host[D:2 * D], host[2 * D:3 * D], host[3 * D:]
         for d, lv in enumerate(self.levels):
             lv.nnz = int(nnz[d])
+            lv.band = int(span[d])
             lv.n_pairs, lv.max_pairs = int(npairs[d]), int(pmax[d])
             # the point form costs 2 gathers per pair against one per stored non-zero; long lists
             # (millions of points per cell on coarse levels of large scenes) stay with the Gram
@@ -637,6 +639,7 @@ class Reconstruction(DualMesher):
             b32 = lv.rhs.float()
             sysd.b32 = b32.data_ptr()
             sysd.col_delta = lv.col_delta.data_ptr() if lv.col_delta is not None else None
+            sysd.band = lv.band
         sysd.b64 = lv.rhs.data_ptr()
         sysd.x32, sysd.x64 = lv.x32.data_ptr(), lv.x64.data_ptr()
         cfg = item.cfg

@@ -118,3 +118,38 @@ def test_stencil_is_symmetric_and_annihilates_nothing():
     assert st[2, 2, 2] > 0
     # the stiffness annihilates constants on a full lattice: its stencil sums to zero
     assert abs(st.sum()) < 1e-12
+
+
+def test_ctypes_structures_match_the_header_layout(tmp_path):
+    """Every structure the Python side passes through the C ABI has the header's size and field
+    offsets: a C program built from include/ngs.h prints them, the ctypes mirrors are compared."""
+    import ctypes
+    import shutil
+    import subprocess
+    import sys
+    sys.path.insert(0, str(ROOT / "neural-galerkin_b200"))
+    from jspsr import _lib as L
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"ngs_grid": L.Grid, "ngs_hash_table": L.HashTable, "ngs_pcg_operator": L.PcgOperator,
+               "ngs_pcg_system": L.PcgSystem, "ngs_pcg_config": L.PcgConfig, "ngs_pcg_batch_item": L.PcgBatchItem}
+    lines = ['#include <stdio.h>', '#include "ngs.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    want = {}
+    for line in filter(None, out):
+        cname, field, value = line.split()
+        want[(cname, field)] = int(value)
+    for cname, py in mirrors.items():
+        assert ctypes.sizeof(py) == want[(cname, "size")], cname
+        for fname, _ in py._fields_:
+            assert getattr(py, fname).offset == want[(cname, fname)], (cname, fname)
