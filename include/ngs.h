@@ -168,6 +168,10 @@ int ngs_grid_finalize(ngs_grid g, void* ws, size_t ws_bytes, int64_t* count_dev,
 int ngs_grid_emit_coords(ngs_grid g, int32_t* coords, ngs_stream s);
 /* rows[i] = row of coords[i] (int32 [n,3]) or -1. */
 int ngs_grid_lookup(ngs_grid g, const int32_t* coords, int64_t n, int64_t* rows, ngs_stream s);
+/* *out_dev (int64) = a bound on |column - row| of the 5^3-stencil matrix over the grid's n set cells
+ * (rows = ranks in (x, y, z) order), from the first rank of every (x, y) column: the value the PCG
+ * takes as ngs_pcg_system.band.  No counterpart in the reference (its solver has no such window). */
+int ngs_grid_band_bound(ngs_grid g, int64_t n, int64_t* out_dev, ngs_stream s);
 
 /* ======================================================================= density / splatting
  * ref: jspsr/core/_hash_backend.py:13-28 (compute_density), :332-356 (splat_data),

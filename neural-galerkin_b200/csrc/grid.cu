@@ -163,6 +163,43 @@ extern "C" int ngs_grid_emit_coords(ngs_grid g, int32_t* coords, ngs_stream s) {
   return NGS_OK;
 }
 
+// A bound on |column - row| of the level's 5^3-stencil matrix from the rank bitmap alone.  Rows are
+// ranks in (x, y, z) order, so the stencil of a voxel of column (x, y) reaches from the first rank of
+// column (x-2, y-2) to the last rank of column (x+2, y+2), while the voxel's own rank lies within
+// column (x, y): per column the larger of the two one-sided spans, then the maximum over columns.
+// The first rank of a column is the scanned rank of its first word.
+__global__ void band_bound_kernel(ngs_grid g, int64_t n, unsigned long long* __restrict__ out) {
+  const GridWord* w = static_cast<const GridWord*>(g.words);
+  const int64_t d0 = g.dims[0], d1 = g.dims[1], zw = g.zwords, ncol = d0 * d1;
+  unsigned long long best = 0;
+  for (int64_t c = ngs_gtid(); c < ncol; c += ngs_gstride()) {
+    const int64_t x = c / d1, y = c - x * d1;
+    const int64_t lo = (x >= 2 ? x - 2 : 0) * d1 + (y >= 2 ? y - 2 : 0);
+    const int64_t hi = (x + 2 < d0 ? x + 2 : d0 - 1) * d1 + (y + 2 < d1 ? y + 2 : d1 - 1) + 1;
+    const int64_t s_c = w[c * zw].rank, s_lo = w[lo * zw].rank;
+    const int64_t s_next = c + 1 < ncol ? (int64_t)w[(c + 1) * zw].rank : n;
+    const int64_t s_hi = hi < ncol ? (int64_t)w[hi * zw].rank : n;
+    const int64_t span = max(s_hi - s_c, s_next - s_lo);
+    if (span > 0 && (unsigned long long)span > best) best = (unsigned long long)span;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+    best = t > best ? t : best;
+  }
+  if ((threadIdx.x & 31) == 0 && best > 0) atomicMax(out, best);
+}
+
+extern "C" int ngs_grid_band_bound(ngs_grid g, int64_t n, int64_t* out_dev, ngs_stream s) {
+  if (!grid_ok(g) || n < 0 || !out_dev) return NGS_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)s;
+  cudaMemsetAsync(out_dev, 0, sizeof(int64_t), st);
+  const int64_t ncol = (int64_t)g.dims[0] * g.dims[1];
+  { ngs_count_launch(); band_bound_kernel<<<ngs_blocks(ncol, 256), 256, 0, st>>>(g, n, reinterpret_cast<unsigned long long*>(out_dev)); }
+  NGS_CHECK_LAUNCH();
+  return NGS_OK;
+}
+
 extern "C" int ngs_grid_lookup(ngs_grid g, const int32_t* coords, int64_t n, int64_t* rows, ngs_stream s) {
   if (!grid_ok(g) || n < 0 || (n > 0 && (!coords || !rows))) return NGS_ERR_INVALID_ARG;
   if (n == 0) return NGS_OK;

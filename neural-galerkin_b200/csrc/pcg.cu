@@ -798,10 +798,14 @@ static int pcg_occupancy(const void* f) {
   return v;
 }
 
+// Cached per device (the occupancy queries and attribute settings behind it cost tens of
+// microseconds of host time, and every solve asks).
 template <int MODE>
 static int pcg_capacity() {
+  static int cached[64];
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && cached[dev] > 0) return cached[dev];
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int per_sm = pcg_occupancy((const void*)pcg_kernel<MODE, PCG_OPS_CSR>);
   per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_CSR>));
@@ -811,7 +815,9 @@ static int pcg_capacity() {
     per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_BOTH>));
   }
   const int64_t cap = (int64_t)sms * per_sm;
-  return (int)(cap < PCG_MAX_BLOCKS ? cap : PCG_MAX_BLOCKS);   // the partials area holds this many blocks
+  const int out = (int)(cap < PCG_MAX_BLOCKS ? cap : PCG_MAX_BLOCKS);   // the partials area holds this many
+  if (dev >= 0 && dev < 64 && out > 0) cached[dev] = out;
+  return out;
 }
 
 // Blocks one solve uses: as many co-resident blocks as fit, fewer for small systems (about

@@ -85,6 +85,7 @@ _SIGS = {
     "ngs_grid_workspace_bytes": ([C.POINTER(Grid)], sz),
     "ngs_grid_finalize": ([G, vp, sz, vp, vp], C.c_int),
     "ngs_grid_emit_coords": ([G, vp, vp], C.c_int),
+    "ngs_grid_band_bound": ([G, i64, vp, vp], C.c_int),
     "ngs_grid_lookup": ([G, vp, i64, vp, vp], C.c_int),
     "ngs_grid_neighbours_tiles": ([i64], i64),
     "ngs_grid_neighbours_count": ([G, vp, vp, C.c_int, i64, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp,

@@ -551,21 +551,14 @@ class Reconstruction(DualMesher):
 
     @staticmethod
     def _row_span_bound(lv: Level) -> torch.Tensor:
-        """Device scalar >= max |column - row| of the level's 5^3-stencil matrix.  Rows are ranks in
-        (x, y, z) order, so the stencil of a voxel in column (x, y) reaches from the first row of
-        column (x-2, y-2) to the last row of column (x+2, y+2), while the voxel's own row lies within
-        column (x, y): the bound is the larger of the two one-sided spans, read from the first rank of
-        every (x, y) column of the bitmap."""
-        g = lv.grid
-        d0, d1, zw = int(g.dims[0]), int(g.dims[1]), int(g.zwords)
-        first = lv.words.view(torch.int32).view(-1, 4)[::zw, 0][:d0 * d1].long()
-        starts = torch.cat([first, torch.full((1,), lv.n, dtype=torch.int64, device=first.device)])
-        x = torch.arange(d0, device=first.device)[:, None]
-        y = torch.arange(d1, device=first.device)[None, :]
-        own = x * d1 + y
-        lo = (x - 2).clamp(min=0) * d1 + (y - 2).clamp(min=0)
-        hi = (x + 2).clamp(max=d0 - 1) * d1 + (y + 2).clamp(max=d1 - 1) + 1
-        return torch.maximum((starts[hi] - starts[own]).max(), (starts[own + 1] - starts[lo]).max())
+        """Device scalar (int64) >= max |column - row| of the level's 5^3-stencil matrix, from the rank
+        bitmap alone (``ngs_grid_band_bound``: rows are ranks in (x, y, z) order, so the stencil of a
+        voxel in column (x, y) reaches from the first row of column (x-2, y-2) to the last row of
+        column (x+2, y+2)).  It decides the 2-byte column deltas and the solver's vector window."""
+        out = torch.zeros((), dtype=torch.int64, device=lv.words.device)
+        if lv.n > 0:
+            L.call("ngs_grid_band_bound", lv.grid, lv.n, L.ptr(out), L.stream())
+        return out
 
     # ------------------------------------------------------------------ RHS + solve
     def _rhs(self, d):

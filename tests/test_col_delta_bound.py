@@ -1,11 +1,14 @@
-"""The bound on |column - row| that decides whether a level's solver reads 2-byte column deltas.
+"""The bound on |column - row| that decides a level's 2-byte column deltas and the solver's vector
+window.
 
-``Reconstruction._row_span_bound`` works from the rank bitmap alone (the first rank of every (x, y)
-column);
-here it runs on CPU over bitmaps built from the oracle's voxel sets and must cover every entry of
-the oracle's matrices of the same levels.
+``ngs_grid_band_bound`` (behind ``Reconstruction._row_span_bound``) works from the rank bitmap alone:
+the first rank of every (x, y) column.  Its rule is restated here in numpy; on CPU the restatement,
+over bitmaps built from the oracle's voxel sets, must cover every entry of the oracle's matrices of
+the same levels and stay close to the largest one; on the GPU the kernel must give the restatement's
+value exactly.
 """
 import numpy as np
+import pytest
 import torch
 
 from oracle import fast as F
@@ -35,17 +38,50 @@ def _bitmap_words(coords, stride):
     return torch.from_numpy(words.reshape(-1)), g
 
 
-def test_row_span_bound_covers_every_column():
+def band_bound(words, g, n):
+    """The kernel's rule: per (x, y) column the larger of (first rank of column (x+2, y+2) + 1 -
+    first rank of the column) and (first rank of the next column - first rank of column (x-2, y-2)),
+    the maximum over columns; the first rank past the last column is n."""
+    d0, d1, zw = g.dims[0], g.dims[1], g.zwords
+    first = words.numpy().reshape(-1, 2)[::zw, 0][:d0 * d1].astype(np.int64)
+    starts = np.concatenate([first, [n]])
+    x = np.arange(d0)[:, None]
+    y = np.arange(d1)[None, :]
+    own = x * d1 + y
+    lo = np.clip(x - 2, 0, None) * d1 + np.clip(y - 2, 0, None)
+    hi = np.clip(x + 2, None, d0 - 1) * d1 + np.clip(y + 2, None, d1 - 1) + 1
+    return int(max((starts[hi] - starts[own]).max(), (starts[own + 1] - starts[lo]).max()))
+
+
+def oracle_levels():
     from jspsr import synthetic
-    from jspsr.core.pipeline import Level, Reconstruction
     xyz, nrm, _ = synthetic.superquadrics(20000, k=2, seed=3)
     r = F.reconstruct(xyz, nrm, 1 / 256, 3, 0.7, 4.0, cg_tol=1e-6, mesh=False)
     for d in range(3):
-        coords, rp, cols = r[f"coords{d}"], r[f"rowptr{d}"], r[f"cols{d}"]
-        words, g = _bitmap_words(coords.astype(np.int64), 1 << d)
-        lv = Level(stride=1 << d, grid=g, words=words, n=coords.shape[0])
-        bound = int(Reconstruction._row_span_bound(lv))
+        yield d, r[f"coords{d}"].astype(np.int64), r[f"rowptr{d}"], r[f"cols{d}"]
+
+
+def test_row_span_bound_covers_every_column():
+    for d, coords, rp, cols in oracle_levels():
+        words, g = _bitmap_words(coords, 1 << d)
+        bound = band_bound(words, g, coords.shape[0])
         rows = np.repeat(np.arange(coords.shape[0]), np.diff(rp))
         actual = int(np.abs(cols - rows).max())
         assert actual <= bound, (d, actual, bound)
         assert bound <= 1.25 * actual + 64, (d, actual, bound)    # and it is tight enough to use
+
+
+@pytest.mark.gpu
+def test_band_bound_kernel_equals_the_rule():
+    from jspsr import _lib as L
+    from jspsr.core.pipeline import Level, Reconstruction
+    dev = torch.device("cuda", 0)
+    for d, coords, _, _ in oracle_levels():
+        words, g = _bitmap_words(coords, 1 << d)
+        stride = 1 << d
+        lo = coords.min(0) // stride * stride
+        grid, dwords = L.make_grid(lo, g.dims, stride, dev)
+        dwords.copy_(words.to(dev))
+        lv = Level(stride=stride, grid=grid, words=dwords, n=coords.shape[0])
+        got = int(Reconstruction._row_span_bound(lv))
+        assert got == band_bound(words, g, coords.shape[0]), d
