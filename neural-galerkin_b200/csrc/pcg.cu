@@ -786,7 +786,9 @@ extern "C" size_t ngs_pcg_workspace_bytes(int64_t n, int mode) {
 // Co-resident blocks of the cooperative kernels on the current device: the fewest over every
 // instantiation a solve of this mode may launch (single, batched; CSR, matrix-free, both).
 // A PCG kernel runs with PCG_WIN_BYTES of dynamic shared memory (the vector window) or none; the
-// occupancy queries assume the window, so that the capacity holds for either launch.
+// occupancy queries assume the window, so that the capacity holds for either launch.  The attribute
+// is set by those queries (the capacity of the cooperative kernels, the cluster limit of the cluster
+// kernels), which are cached per device and which every launch path calls before it launches.
 static void pcg_smem_attr(const void* f) {
   cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, PCG_WIN_BYTES);
 }
@@ -946,7 +948,6 @@ static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
   void* args[] = {&a};
   ngs_count_launch();
   const void* f = pcg_cluster_kernel_of(mode, a.mf != 0);
-  pcg_smem_attr(f);
   const cudaError_t e = cudaLaunchKernelExC(&lc, f, args);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
@@ -1080,7 +1081,6 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   void* args[] = {&a};
   ngs_count_launch();
   void* f = pcg_kernel_of(cfg->mode, a.mf != 0);
-  pcg_smem_attr(f);
   const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3((unsigned)blocks), dim3(PCG_THREADS), args, pcg_win_smem(a),
                                                     st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
@@ -1152,7 +1152,6 @@ extern "C" int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items,
   void* args[] = {&b};
   ngs_count_launch();
   void* f = pcg_batch_kernel_of(mode, ops);
-  pcg_smem_attr(f);
   const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3(total), dim3(PCG_THREADS), args, smem, st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
