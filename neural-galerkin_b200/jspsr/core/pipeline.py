@@ -814,42 +814,46 @@ class Reconstruction(DualMesher):
         max_depth = self.depth
         q = [np.float32(self.bbox[:3]) * np.float32(self.inv_vs), np.float32(self.bbox[3:]) * np.float32(self.inv_vs)]
         base, leaf_flags, parent_grids = {}, {}, {}
-        for d in range(max_depth):
+        # parents at 2s of every level's voxels (but the coarsest), their counts read in one go
+        pcount = torch.empty(max(max_depth - 1, 1), dtype=torch.int64, device=dev)
+        for d in range(max_depth - 1):
             lv = self.levels[d]
-            s = lv.stride
+            lo, dims = _box(q[0], q[1], 2 * lv.stride, pad=2)
+            pg, pw = L.make_grid(lo, dims, 2 * lv.stride, dev)
+            L.call("ngs_grid_mark_coords", pg, L.ptr(lv.coords), lv.n, None, 1, 0, st)
+            parent_grids[d] = (pg, pw, L.grid_finalize(pg, pw, pcount[d:d + 1]))
+        npar = pcount.cpu().numpy()
+        if not self._status_checked:
+            # first synchronisation after the solves: their status copy has landed; a failed solve
+            # raises here, before any mesh is built from its result
+            self.check_solves()
+        # each level's cells: all 8 children of its parents (the coarsest level: its voxels), and on
+        # levels above 0 the flags of the leaves among them; the leaf counts read in one go
+        ltot = []
+        for d in range(max_depth):
             if d < max_depth - 1:
-                # parents at 2s of the level's voxels, then all 8 children of each parent
-                lo, dims = _box(q[0], q[1], 2 * s, pad=2)
-                pg, pw = L.make_grid(lo, dims, 2 * s, dev)
-                L.call("ngs_grid_mark_coords", pg, L.ptr(lv.coords), lv.n, None, 1, 0, st)
-                pc = torch.empty(1, dtype=torch.int64, device=dev)
-                ws = L.grid_finalize(pg, pw, pc)
-                npar = int(pc.item())
-                if not self._status_checked:
-                    # first synchronisation after the solves: their status copy has landed; a failed
-                    # solve raises here, before any mesh is built from its result
-                    self.check_solves()
-                parents = torch.empty((npar, 3), dtype=torch.int32, device=dev)
+                pg = parent_grids[d][0]
+                parents = torch.empty((int(npar[d]), 3), dtype=torch.int32, device=dev)
                 L.call("ngs_grid_emit_coords", pg, L.ptr(parents), st)
-                cells = torch.empty((npar * 8, 3), dtype=torch.int32, device=dev)
-                L.call("ngs_conformal_children", L.ptr(parents), npar, s, L.ptr(cells), st)
-                parent_grids[d] = (pg, pw, ws)
+                cells = torch.empty((int(npar[d]) * 8, 3), dtype=torch.int32, device=dev)
+                L.call("ngs_conformal_children", L.ptr(parents), int(npar[d]), self.levels[d].stride, L.ptr(cells), st)
             else:
-                cells = lv.coords
+                cells = self.levels[d].coords
             if d > 0:
                 leaf = torch.empty(cells.shape[0], dtype=torch.int32, device=dev)
-                pg = parent_grids[d - 1][0]
-                L.call("ngs_leaf_flags", L.ptr(cells), cells.shape[0], pg, L.ptr(leaf), st)
+                L.call("ngs_leaf_flags", L.ptr(cells), cells.shape[0], parent_grids[d - 1][0], L.ptr(leaf), st)
                 off, tot = L.scan(leaf)
-                nleaf = int(tot.item())
-                if nleaf == 0:
-                    max_depth = d
-                    break
-                leaf_flags[d] = (leaf, off, nleaf)
+                leaf_flags[d] = (leaf, off)
+                ltot.append(tot)
             base[d] = cells
+        nleaf = torch.cat(ltot).cpu().numpy() if ltot else np.zeros(0, np.int64)
         for d in range(1, max_depth):
-            leaf, off, nleaf = leaf_flags[d]
-            out = torch.empty((nleaf, 3), dtype=torch.int32, device=dev)
+            if int(nleaf[d - 1]) == 0:          # no leaves from level d on: the mesh stops at d - 1
+                max_depth = d
+                break
+        for d in range(1, max_depth):
+            leaf, off = leaf_flags[d]
+            out = torch.empty((int(nleaf[d - 1]), 3), dtype=torch.int32, device=dev)
             L.call("ngs_compact_coords", L.ptr(base[d]), L.ptr(leaf), L.ptr(off), base[d].shape[0], L.ptr(out), st)
             base[d] = out
         self._mark("leaves")
