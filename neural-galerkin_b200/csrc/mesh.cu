@@ -310,38 +310,76 @@ __global__ void dual_count_kernel(const int32_t* __restrict__ acc, int W, const 
   }
 }
 
-__global__ void dual_emit_kernel(const int32_t* __restrict__ acc, int W, const int32_t* __restrict__ cnt, int64_t m,
-                                 const float* __restrict__ pos, const float* __restrict__ values,
-                                 const int64_t* __restrict__ voff, float* __restrict__ tris,
-                                 int32_t* __restrict__ vids) {
-  for (int64_t c = ngs_gtid(); c < m; c += ngs_gstride()) {
-    // voff is the exclusive scan of the count pass: a cube without vertices (most of them) is
-    // recognised from two neighbouring offsets, without reading its corners
-    const int64_t base = voff[c];
-    if (c + 1 < m && voff[c + 1] == base) continue;
-    if (cnt && cnt[c] != 8) continue;
-    int id[8];
-    float v[8];
+// A warp per 32 consecutive cubes.  A thread per cube would leave most lanes idle (most cubes have
+// no vertices: 6 of 32 lanes active on average).  Here each lane stages the corner ids, values and
+// case of its own cube, if it emits, in shared memory; then the warp takes its cubes' vertices --
+// contiguous in the output, since voff is the exclusive scan of the count pass -- 32 at a time:
+// vertex j belongs to the last lane whose start offset is at most j (a binary search over the
+// lanes' offsets by shuffles), as its k-th vertex, edge c_tri[case][k].
+constexpr int EMIT_WARPS = 4;
+
+__global__ void __launch_bounds__(EMIT_WARPS * 32) dual_emit_kernel(
+    const int32_t* __restrict__ acc, int W, const int32_t* __restrict__ cnt, int64_t m, const float* __restrict__ pos,
+    const float* __restrict__ values, const int64_t* __restrict__ voff, float* __restrict__ tris,
+    int32_t* __restrict__ vids) {
+  __shared__ int s_id[EMIT_WARPS][32][8];
+  __shared__ float s_v[EMIT_WARPS][32][8];
+  __shared__ int s_t[EMIT_WARPS][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t chunks = (m + 31) / 32, step = (int64_t)gridDim.x * EMIT_WARPS;
+  for (int64_t ch = (int64_t)blockIdx.x * EMIT_WARPS + w; ch < chunks; ch += step) {
+    const int64_t c = ch * 32 + lane;
+    const bool in = c < m;
+    const int64_t start = in ? voff[c] : 0;
+    // a cube emits if its count-pass range is not empty (the last cube: always looked at)
+    bool active = in && !(c + 1 < m && voff[c + 1] == start) && !(cnt && cnt[c] != 8);
+    int nv = 0;
+    if (active) {
+      float v[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      id[i] = acc[(c * 8 + i) * W];
-      v[i] = values[id[i]];
+      for (int i = 0; i < 8; i++) {
+        const int id = acc[(c * 8 + i) * W];
+        v[i] = values[id];
+        s_id[w][lane][i] = id;
+        s_v[w][lane][i] = v[i];
+      }
+      const int t = cube_type(v);
+      s_t[w][lane] = t;
+      nv = num_verts(t);
     }
-    const int t = cube_type(v);
-    for (int k = 0; k < 16 && c_tri[t][k] >= 0; k++) {
-      const int e = c_tri[t][k];
-      const int a = c_edge[e][0], b = c_edge[e][1];
-      const float p1[3] = {pos[id[a] * 3], pos[id[a] * 3 + 1], pos[id[a] * 3 + 2]};
-      const float p2[3] = {pos[id[b] * 3], pos[id[b] * 3 + 1], pos[id[b] * 3 + 2]};
-      float out[3];
-      sdf_interp(p1, p2, v[a], v[b], out);
-      const int64_t o = base + k;
-      tris[o * 3] = out[0];
-      tris[o * 3 + 1] = out[1];
-      tris[o * 3 + 2] = out[2];
-      vids[o * 2] = max(id[a], id[b]);
-      vids[o * 2 + 1] = min(id[a], id[b]);
+    const int64_t first = __shfl_sync(0xffffffffu, start, 0);
+    const int rel = in ? (int)(start - first) : 0x7fffffff;      // this lane's first vertex in the warp's range
+    int total = nv;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    __syncwarp();
+    for (int j0 = 0; j0 < total; j0 += 32) {                   // warp-uniform trip count
+      const int j = j0 + lane;
+      int L = 0;
+#pragma unroll
+      for (int sstep = 16; sstep > 0; sstep >>= 1) {
+        const int r = __shfl_sync(0xffffffffu, rel, L + sstep);
+        if (r <= j) L += sstep;
+      }
+      const int rL = __shfl_sync(0xffffffffu, rel, L);
+      if (j < total) {
+        const int k = j - rL;
+        const int e = c_tri[s_t[w][L]][k];
+        const int a = c_edge[e][0], b = c_edge[e][1];
+        const int ia = s_id[w][L][a], ib = s_id[w][L][b];
+        const float p1[3] = {pos[(int64_t)ia * 3], pos[(int64_t)ia * 3 + 1], pos[(int64_t)ia * 3 + 2]};
+        const float p2[3] = {pos[(int64_t)ib * 3], pos[(int64_t)ib * 3 + 1], pos[(int64_t)ib * 3 + 2]};
+        float out[3];
+        sdf_interp(p1, p2, s_v[w][L][a], s_v[w][L][b], out);
+        const int64_t o = first + j;
+        tris[o * 3] = out[0];
+        tris[o * 3 + 1] = out[1];
+        tris[o * 3 + 2] = out[2];
+        vids[o * 2] = max(ia, ib);
+        vids[o * 2 + 1] = min(ia, ib);
+      }
     }
+    __syncwarp();                                                // the next chunk overwrites the stage
   }
 }
 
@@ -363,7 +401,7 @@ extern "C" int ngs_dual_mc_emit(const int32_t* acc, int slot_words, const int32_
     return NGS_ERR_INVALID_ARG;
   if (slot_words != 1 && slot_words != 2) return NGS_ERR_INVALID_ARG;
   if (n_cubes == 0) return NGS_OK;
-  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, 128), 128, 0, (cudaStream_t)s>>>(acc, slot_words, cnt, n_cubes, pos, values,
+  { ngs_count_launch(); dual_emit_kernel<<<ngs_blocks(n_cubes, EMIT_WARPS * 32), EMIT_WARPS * 32, 0, (cudaStream_t)s>>>(acc, slot_words, cnt, n_cubes, pos, values,
                                                                                              voffset, tris, vert_ids); }
   NGS_CHECK_LAUNCH();
   return NGS_OK;
