@@ -456,18 +456,45 @@ NGS_DEV void vd_rank_sort(int64_t s0, int c, int lane, int64_t* __restrict__ sor
   __syncwarp();
 }
 
+// A bucket of at most 8 keys sorted by the lane that owns it: the keys in registers, Batcher's
+// 19-comparator odd-even merge network (empty slots hold INT64_MAX and stay at the end), then the
+// sorted keys and the first-of-vid1 flags written back.
+constexpr int VD_LANE_MAX = 8;
+NGS_DEV void vd_lane_sort(int64_t s0, int c, int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
+  int64_t k[VD_LANE_MAX];
+#pragma unroll
+  for (int i = 0; i < VD_LANE_MAX; i++) k[i] = i < c ? sorted[s0 + i] : INT64_MAX;
+  constexpr int net[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {1, 2}, {5, 6},
+                              {0, 4}, {1, 5}, {2, 6}, {3, 7}, {2, 4}, {3, 5}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+  for (int q = 0; q < 19; q++) {
+    const int64_t a = k[net[q][0]], b = k[net[q][1]];
+    k[net[q][0]] = a < b ? a : b;
+    k[net[q][1]] = a < b ? b : a;
+  }
+#pragma unroll
+  for (int i = 0; i < VD_LANE_MAX; i++) {
+    if (i < c) {
+      sorted[s0 + i] = k[i];
+      first[s0 + i] = (i == 0 || (k[i] >> 32) != (k[i - 1 > 0 ? i - 1 : 0] >> 32)) ? 1 : 0;
+    }
+  }
+}
+
 __global__ void vd_sort_kernel(const int64_t* __restrict__ start, const int32_t* __restrict__ count, int64_t nb,
                                int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
   const int lane = threadIdx.x & 31;
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  // a warp reads 32 bucket counts at once (most buckets are empty or hold one key), then sorts the
-  // buckets of 2..512 keys among them one after the other
+  // a warp reads 32 bucket counts at once (most buckets are empty or hold a few keys); the buckets of
+  // 2..8 keys are sorted by their own lanes at once, those of 9..512 keys by the whole warp one after
+  // the other
   for (int64_t base = warp0 * 32; base < nb; base += nwarps * 32) {
     const int64_t b = base + lane;
     const int c = b < nb ? count[b] : 0;
     if (c == 1) first[start[b]] = 1;
-    unsigned todo = __ballot_sync(0xffffffffu, c >= 2 && c <= 512);
+    else if (c >= 2 && c <= VD_LANE_MAX) vd_lane_sort(start[b], c, sorted, first);
+    unsigned todo = __ballot_sync(0xffffffffu, c > VD_LANE_MAX && c <= 512);
     while (todo) {
       const int src = __ffs(todo) - 1;
       todo &= todo - 1;
