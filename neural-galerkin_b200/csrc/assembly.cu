@@ -477,7 +477,9 @@ extern "C" int ngs_rhs_normals(ngs_grid data_grid, const int32_t* data_coords, i
 // ----------------------------------------------------------------------------- cross-level correction
 // rhs_fine[i] -= sum over the 125 coarse neighbours j of K(i, j) * x_coarse[j]
 // (reconstructor.py:153-168, stiffness part; computed matrix-free).
-__global__ void correction_kernel(const int32_t* __restrict__ fc, int64_t nf, int sf, ngs_grid cg,
+// 64 registers (eight 128-thread blocks per SM, no spills): more resident warps to wait on the bitmap
+// runs and gathers (0.89 -> 0.82 ms for the 300k cloud).
+__global__ void __launch_bounds__(128, 8) correction_kernel(const int32_t* __restrict__ fc, int64_t nf, int sf, ngs_grid cg,
                                   const float* __restrict__ x, const double* __restrict__ tc,
                                   const double* __restrict__ tg, int tab_len, double* __restrict__ rhs) {
   extern __shared__ double tabs[];

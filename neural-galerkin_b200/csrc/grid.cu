@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(128, 6) eval_field_levels_kernel(const __grid_
 // are at least half the leaf cell's size, the two positions of an axis fall in the same or in
 // adjacent field cells, so the 8 samples' 27-cell neighbourhoods lie in one 4 x 4 x 4 box.  The box
 // is looked up once (16 runs of 4 cells along z) and the tensor-product sums are contracted axis by
-// axis in registers -- z while the box is read (2 x 16 sums), then y (16), then x (8 samples) --
+// axis in registers -- z while the box is read, y per x slab of the box, then x (8 samples) --
 // with each sample's three basis values placed at its offset in a 4-wide weight vector.  That is
 // 224 multiply-adds per cell and level instead of 8 x 27 triple products.  Levels whose cells are
 // smaller take the per-sample path.  Levels are added in level order.
@@ -521,7 +521,13 @@ __device__ __noinline__ float sample_field(const ngs_grid& g, const float* p, fl
   return v;
 }
 
-__global__ void __launch_bounds__(128) field_cells_kernel(const __grid_constant__ FieldLevels fl,
+// w[i] for a thread-dependent i, by selects (an indexed register array would go to local memory).
+NGS_DEV float sel4(const float (&w)[4], int i) { return i == 0 ? w[0] : i == 1 ? w[1] : i == 2 ? w[2] : w[3]; }
+
+// Eight 128-thread blocks per SM (64 registers, a few spilled to L1): the kernel waits on its bitmap
+// runs and gathers, and twice the resident warps hide more of that than the spills cost (2.1 -> 1.6
+// ms for the 300k cloud's mesh samples).
+__global__ void __launch_bounds__(128, 8) field_cells_kernel(const __grid_constant__ FieldLevels fl,
                                                           int64_t n_cells, const float* __restrict__ pos,
                                                           float inv_vs, double vs, float* __restrict__ out) {
   for (int64_t c = ngs_gtid(); c < n_cells; c += ngs_gstride()) {
@@ -568,10 +574,15 @@ __global__ void __launch_bounds__(128) field_cells_kernel(const __grid_constant_
         for (int e = 0; e < 8; e++) acc[e] += sample_field(g, P + e * 3, inv_vs, vs, x);
         continue;
       }
-      // z contraction while reading the box: cz[tz][ix][iy]
-      float cz[2][4][4];
+      // one x slab of the box at a time (its 4 runs of 4 cells along z in flight together): z sums
+      // while the runs are read, folded into the slab's y sums, which go into the x sums -- each sum
+      // in the same order as a contraction of the whole box axis by axis
+      float xs[8];
 #pragma unroll
-      for (int ix = 0; ix < 4; ix++)
+      for (int e = 0; e < 8; e++) xs[e] = 0.f;
+#pragma unroll 1
+      for (int ix = 0; ix < 4; ix++) {
+        float cy[2][2] = {{0.f, 0.f}, {0.f, 0.f}};             // [tz][ty]
 #pragma unroll
         for (int iy = 0; iy < 4; iy++) {
           int32_t r[4];
@@ -584,29 +595,21 @@ __global__ void __launch_bounds__(128) field_cells_kernel(const __grid_constant_
             float sum = 0.f;
 #pragma unroll
             for (int iz = 0; iz < 4; iz++) sum += w[2][tz][iz] * xv[iz];
-            cz[tz][ix][iy] = sum;
+#pragma unroll
+            for (int ty = 0; ty < 2; ty++) cy[tz][ty] += w[1][ty][iy] * sum;
           }
         }
 #pragma unroll
-      for (int tz = 0; tz < 2; tz++)
+        for (int tx = 0; tx < 2; tx++) {
+          const float wx = sel4(w[0][tx], ix);
 #pragma unroll
-        for (int ty = 0; ty < 2; ty++) {
-          float cy[4];
+          for (int ty = 0; ty < 2; ty++)
 #pragma unroll
-          for (int ix = 0; ix < 4; ix++) {
-            float sum = 0.f;
-#pragma unroll
-            for (int iy = 0; iy < 4; iy++) sum += w[1][ty][iy] * cz[tz][ix][iy];
-            cy[ix] = sum;
-          }
-#pragma unroll
-          for (int tx = 0; tx < 2; tx++) {
-            float sum = 0.f;
-#pragma unroll
-            for (int ix = 0; ix < 4; ix++) sum += w[0][tx][ix] * cy[ix];
-            acc[tx * 4 + ty * 2 + tz] += sum;
-          }
+            for (int tz = 0; tz < 2; tz++) xs[tx * 4 + ty * 2 + tz] += wx * cy[tz][ty];
         }
+      }
+#pragma unroll
+      for (int e = 0; e < 8; e++) acc[e] += xs[e];
     }
 #pragma unroll
     for (int e = 0; e < 8; e++) out[c * 8 + e] = acc[e];

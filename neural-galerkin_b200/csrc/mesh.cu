@@ -481,7 +481,7 @@ NGS_DEV void vd_lane_sort(int64_t s0, int c, int64_t* __restrict__ sorted, int32
   }
 }
 
-__global__ void vd_sort_kernel(const int64_t* __restrict__ start, const int32_t* __restrict__ count, int64_t nb,
+__global__ void __launch_bounds__(256, 4) vd_sort_kernel(const int64_t* __restrict__ start, const int32_t* __restrict__ count, int64_t nb,
                                int64_t* __restrict__ sorted, int32_t* __restrict__ first) {
   const int lane = threadIdx.x & 31;
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
