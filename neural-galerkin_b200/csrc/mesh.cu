@@ -190,14 +190,16 @@ __global__ void dual_inds_cells_kernel(ngs_grid dual, const int32_t* __restrict_
   for (int64_t i = ngs_gtid(); i < n; i += ngs_gstride()) {
     const int x0 = cells[i * 3] * 2, y0 = cells[i * 3 + 1] * 2, z0 = cells[i * 3 + 2] * 2;
     const int64_t id0 = idx_base + i * 8;
-#pragma unroll 1
+    // the 9 runs looked up first, all their bitmap loads in flight together, then the updates
+    int32_t r[9][3];
+#pragma unroll
+    for (int pxy = 0; pxy < 9; pxy++) grid_rows_zrun<3>(dual, x0 + pxy / 3, y0 + pxy % 3, z0, r[pxy]);
+#pragma unroll
     for (int pxy = 0; pxy < 9; pxy++) {
       const int px = pxy / 3, py = pxy % 3;
-      int32_t r[3];
-      grid_rows_zrun<3>(dual, x0 + px, y0 + py, z0, r);
 #pragma unroll
       for (int pz = 0; pz < 3; pz++) {
-        const int64_t row = r[pz];
+        const int64_t row = r[pxy][pz];
         if (row < 0) continue;
         const int nx = px == 1 ? 2 : 1, ny = py == 1 ? 2 : 1, nz = pz == 1 ? 2 : 1;
         atomicAdd(cnt + row, nx * ny * nz);
