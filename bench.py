@@ -512,7 +512,7 @@ def main():
             if line.startswith("dram_bytes_per_iteration_level0:"):
                 traffic = float(line.split(":")[1]) * iters0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "pcg_kernel<MIXED> (level 0)",
+                "traffic": traffic, "kernel": "pcg_form_kernel<MIXED> (level 0)",
                 "peak_source": "measured" if pk.exists() else "fallback",
                 "bytes_per_launch": alg_bytes, "launch_ms": pcg_ms[0], "iterations": iters0}
 

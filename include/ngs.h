@@ -322,7 +322,9 @@ typedef struct ngs_pcg_system {
   float* x32;                /* [n] out (REFERENCE, MIXED: FP32 copy of x) */
   double* x64;               /* [n] out (MIXED, FP64) */
   const int16_t* col_delta;  /* [nnz] optional: column - row of every entry; when given the solver
-                                reads these 2-byte deltas instead of the 4-byte columns (NULL: cols) */
+                                reads these 2-byte deltas instead of the 4-byte columns in the
+                                launches that use its shared-memory window (see band), and the
+                                4-byte columns, if given too, in the others (NULL: cols) */
   const ngs_pcg_operator* op;/* optional: matrix-free operator instead of the CSR (NULL: CSR) */
   int64_t band;              /* optional: a bound on |column - row| over the matrix, for a CSR whose
                                 columns increase within every row (0: unknown, or unsorted rows).
@@ -374,6 +376,10 @@ typedef struct ngs_pcg_batch_item {
  * enough for one thread-block cluster and is solved by its own cluster launch, alone or in a batch --
  * ngs_pcg_cluster_size gives the CTAs of that cluster, 0 for the cooperative path). */
 int ngs_pcg_block_capacity(int mode);
+/* 1 if a solve of a system of n rows, nnz non-zeros and bandwidth bound band (as
+ * ngs_pcg_system.band) stages its search vector in shared memory -- the launches in which the solver
+ * reads 2-byte column deltas -- else 0.  No counterpart in the reference. */
+int ngs_pcg_window(int64_t n, int64_t nnz, int64_t band, int mode);
 int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode);
 int ngs_pcg_cluster_size(int64_t n, int64_t nnz, int mode);
 int ngs_pcg_solve_batch(const ngs_pcg_batch_item* items, int n_items, ngs_stream s);

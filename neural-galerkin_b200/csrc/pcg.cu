@@ -257,12 +257,27 @@ NGS_DEV void spmv_rows_plain(const PcgArgs& a, const MT* __restrict__ vals, cons
   __syncthreads();
 }
 // The streaming choice is a template argument: one load form per instantiation (a runtime choice
-// per load cost 7 % of the level-0 solve and forced register spills).
-template <typename MT, typename VT, typename ACC, typename Pre, typename Epi>
+// per load cost 7 % of the level-0 solve and forced register spills).  FORM picks the SpMV form at
+// compile time (kernels specialised per form, so that one form's register allocation is not shaped
+// by the others') or, with PCG_FORM_ANY, at run time from the system (one kernel for every system of
+// a batch or a cluster launch).  Each form runs the same uncontracted arithmetic in every kernel, so
+// a system's result does not depend on which kernel solved it.
+constexpr int PCG_FORM_ANY = 0, PCG_FORM_DELTA_STREAM = 1, PCG_FORM_DELTA = 2, PCG_FORM_COLS_STREAM = 3,
+              PCG_FORM_COLS = 4;
+
+template <int FORM, typename MT, typename VT, typename ACC, typename Pre, typename Epi>
 NGS_DEV void spmv_rows(const PcgArgs& a, const MT* __restrict__ vals, const VT* v, int64_t voff, int64_t row0,
                        int64_t row1, Pre pre, Epi epi, double& dsum) {
-  // the column encoding too: 2-byte deltas when the caller supplied them, 4-byte columns otherwise
-  if (a.cols16) {
+  if constexpr (FORM == PCG_FORM_DELTA_STREAM) {
+    spmv_rows_piped<true, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+  } else if constexpr (FORM == PCG_FORM_DELTA) {
+    spmv_rows_piped<false, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+  } else if constexpr (FORM == PCG_FORM_COLS_STREAM) {
+    spmv_rows_plain<true, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+  } else if constexpr (FORM == PCG_FORM_COLS) {
+    spmv_rows_plain<false, false, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
+  } else if (a.cols16) {
+    // the column encoding too: 2-byte deltas when the caller supplied them, 4-byte columns otherwise
     if (a.evict_first) spmv_rows_piped<true, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
     else spmv_rows_piped<false, true, MT, VT, ACC>(a, vals, v, voff, row0, row1, pre, epi, dsum);
   } else {
@@ -504,7 +519,7 @@ NGS_DEV void pcg_abandon(const PcgArgs& a, int it) {
 // register budget of the other operator's code out of the kernel.
 constexpr int PCG_OPS_CSR = 1, PCG_OPS_MF = 2, PCG_OPS_BOTH = 3;
 
-template <int MODE, int OPS, typename Sync>
+template <int MODE, int OPS, int FORM, typename Sync>
 NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   using MT = typename PcgTypes<MODE>::MT;
   using VT = typename PcgTypes<MODE>::VT;
@@ -540,8 +555,8 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
   };
   // the true residual uses the FP64 matrix in MIXED mode, the recurrence matrix otherwise
   auto spmv_true = [&](double& sum) {
-    if constexpr (MODE == NGS_PCG_MIXED) spmv_rows<double, RT, double>(a, a.vals64, x, 0, row0, row1, res_pre, true_res_epi, sum);
-    else spmv_rows<MT, RT, ACC>(a, vals, x, 0, row0, row1, res_pre, true_res_epi, sum);
+    if constexpr (MODE == NGS_PCG_MIXED) spmv_rows<FORM, double, RT, double>(a, a.vals64, x, 0, row0, row1, res_pre, true_res_epi, sum);
+    else spmv_rows<FORM, MT, RT, ACC>(a, vals, x, 0, row0, row1, res_pre, true_res_epi, sum);
   };
   // w = A u: the block's window of u staged in shared memory when it fits (refreshed every product;
   // the grid barrier before the product made every block's u rows visible)
@@ -559,9 +574,9 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
       VT* win = reinterpret_cast<VT*>(pcg_win_raw);
       for (int64_t i = threadIdx.x; i < wn; i += PCG_THREADS) win[i] = u[wlo + i];
       __syncthreads();
-      spmv_rows<MT, VT, ACC>(a, vals, win, wlo, row0, row1, w_pre, w_epi, sum);
+      spmv_rows<FORM, MT, VT, ACC>(a, vals, win, wlo, row0, row1, w_pre, w_epi, sum);
     } else {
-      spmv_rows<MT, VT, ACC>(a, vals, u, 0, row0, row1, w_pre, w_epi, sum);
+      spmv_rows<FORM, MT, VT, ACC>(a, vals, u, 0, row0, row1, w_pre, w_epi, sum);
     }
   };
 
@@ -733,7 +748,14 @@ NGS_DEV void pcg_body(const PcgArgs& a, const unsigned bid, Sync& sy) {
 template <int MODE, int OPS>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_kernel(const __grid_constant__ PcgArgs a) {
   GridSync sy(a, blockIdx.x);
-  pcg_body<MODE, OPS>(a, blockIdx.x, sy);
+  pcg_body<MODE, OPS, PCG_FORM_ANY>(a, blockIdx.x, sy);
+}
+
+// The single-system solve of an assembled matrix with its SpMV form fixed at compile time.
+template <int MODE, int FORM>
+__global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_form_kernel(const __grid_constant__ PcgArgs a) {
+  GridSync sy(a, blockIdx.x);
+  pcg_body<MODE, PCG_OPS_CSR, FORM>(a, blockIdx.x, sy);
 }
 
 // A small system solved by one thread-block cluster (a.nblocks CTAs, the whole grid).
@@ -741,7 +763,7 @@ template <int MODE, int OPS>
 __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_cluster_kernel(const __grid_constant__ PcgArgs a) {
   __shared__ double cred[8], bcast[4];
   ClusterSync sy{cluster_rank(), cluster_size(), cred, bcast, 0, 0ull, a.budget_ns, false};
-  pcg_body<MODE, OPS>(a, sy.rank, sy);
+  pcg_body<MODE, OPS, PCG_FORM_ANY>(a, sy.rank, sy);
   cluster_sync_all();            // no CTA exits while another may still read its shared memory
 }
 
@@ -764,7 +786,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_batch_kernel(
     if (b.start[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
   }
   GridSync sy(b.sys[lo], blockIdx.x - b.start[lo]);
-  pcg_body<MODE, OPS>(b.sys[lo], blockIdx.x - b.start[lo], sy);
+  pcg_body<MODE, OPS, PCG_FORM_ANY>(b.sys[lo], blockIdx.x - b.start[lo], sy);
 }
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -812,6 +834,10 @@ static int pcg_capacity() {
   int per_sm = pcg_occupancy((const void*)pcg_kernel<MODE, PCG_OPS_CSR>);
   per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_CSR>));
   if constexpr (MODE != NGS_PCG_REFERENCE) {
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_form_kernel<MODE, PCG_FORM_DELTA_STREAM>));
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_form_kernel<MODE, PCG_FORM_DELTA>));
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_form_kernel<MODE, PCG_FORM_COLS_STREAM>));
+    per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_form_kernel<MODE, PCG_FORM_COLS>));
     per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_kernel<MODE, PCG_OPS_MF>));
     per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_MF>));
     per_sm = std::min(per_sm, pcg_occupancy((const void*)pcg_batch_kernel<MODE, PCG_OPS_BOTH>));
@@ -901,6 +927,22 @@ extern "C" int ngs_pcg_cluster_size(int64_t n, int64_t nnz, int mode) {
   return pcg_cluster_for(n, nnz, 0, cluster_limit_of(mode));
 }
 
+static void pcg_set_window(PcgArgs& a, int mode, int64_t band, int64_t nblocks);
+
+// Whether a solo solve of such a system stages its search vector in shared memory (the same decision
+// as ngs_pcg_solve), so that a caller builds 2-byte column deltas only where they are read.
+extern "C" int ngs_pcg_window(int64_t n, int64_t nnz, int64_t band, int mode) {
+  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0 || band <= 0) return 0;
+  const int csize = ngs_pcg_cluster_size(n, nnz, mode);
+  const int64_t blocks = csize > 0 ? csize : pcg_blocks_for(n, nnz, 0, capacity_of(mode));
+  if (blocks < 1) return 0;
+  PcgArgs a{};
+  a.n = n;
+  a.nnz = nnz;
+  pcg_set_window(a, mode, band, blocks);
+  return a.win_cap > 0 ? 1 : 0;
+}
+
 extern "C" int ngs_pcg_blocks(int64_t n, int64_t nnz, int mode) {
   if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0) return 0;
   if (ngs_pcg_cluster_size(n, nnz, mode) > 0) return 0;      // solved by a cluster, outside the grid
@@ -920,10 +962,18 @@ static void* pcg_cluster_kernel_of(int mode, bool mf) {
 // the space stays with the L1 cache the gathers hit: a window reserved for blocks that cannot use it
 // cost 7 % of the level-0 solve of a 300k-point cloud (half of its blocks do not fit) and 9 % on a
 // 5M-point room.
+// The column encoding follows: with the window, the 2-byte deltas in the software-pipelined row loop
+// (level 1 of a 300k-point cloud: 3.51 against 3.76 ms with 4-byte columns); without it, the 4-byte
+// columns in the row-at-a-time loop when the caller supplied both (its level 0: 9.22 against 9.34
+// ms).  Solo and batched solves of a system take the same decision, so their results stay identical.
 static void pcg_set_window(PcgArgs& a, int mode, int64_t band, int64_t nblocks) {
   const int64_t cap = PCG_WIN_BYTES / (int64_t)pcg_vec_bytes(mode);
   const int64_t rows = nblocks > 0 ? (a.n + nblocks - 1) / nblocks : a.n;
   a.win_cap = (!a.mf && band > 0 && rows + 2 * band <= cap) ? (int)cap : 0;
+  if (a.win_cap == 0 && a.cols && a.cols16) {
+    a.cols16 = nullptr;
+    a.evict_first = (size_t)a.nnz * (4 + (mode == NGS_PCG_FP64 ? 8 : 4)) > (size_t)96 << 20;
+  }
 }
 
 static size_t pcg_win_smem(const PcgArgs& a) { return a.win_cap > 0 ? PCG_WIN_BYTES : 0; }
@@ -1033,6 +1083,14 @@ static int prepare_pcg(const ngs_pcg_system* sys, const ngs_pcg_config* cfg, voi
   return NGS_OK;
 }
 
+// The single-system kernel of an assembled matrix in the MIXED and FP64 modes: the one specialised
+// for its SpMV form.
+template <int MODE>
+static void* pcg_form_kernel_for(const PcgArgs& a) {
+  if (a.cols16) return a.evict_first ? (void*)pcg_form_kernel<MODE, PCG_FORM_DELTA_STREAM> : (void*)pcg_form_kernel<MODE, PCG_FORM_DELTA>;
+  return a.evict_first ? (void*)pcg_form_kernel<MODE, PCG_FORM_COLS_STREAM> : (void*)pcg_form_kernel<MODE, PCG_FORM_COLS>;
+}
+
 static void* pcg_kernel_of(int mode, bool mf) {
   if (mode == NGS_PCG_REFERENCE) return (void*)pcg_kernel<NGS_PCG_REFERENCE, PCG_OPS_CSR>;
   if (mode == NGS_PCG_MIXED)
@@ -1080,7 +1138,10 @@ extern "C" int ngs_pcg_solve(const ngs_pcg_system* sys, const ngs_pcg_config* cf
   cudaMemsetAsync(a.count, 0, 8 * sizeof(unsigned int), st);
   void* args[] = {&a};
   ngs_count_launch();
-  void* f = pcg_kernel_of(cfg->mode, a.mf != 0);
+  void* f = a.mf ? pcg_kernel_of(cfg->mode, true)
+             : cfg->mode == NGS_PCG_MIXED ? pcg_form_kernel_for<NGS_PCG_MIXED>(a)
+             : cfg->mode == NGS_PCG_FP64 ? pcg_form_kernel_for<NGS_PCG_FP64>(a)
+             : pcg_kernel_of(cfg->mode, false);
   const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3((unsigned)blocks), dim3(PCG_THREADS), args, pcg_win_smem(a),
                                                     st);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);

@@ -135,6 +135,7 @@ _SIGS = {
     "ngs_pcg_solve": ([C.POINTER(PcgSystem), C.POINTER(PcgConfig), vp, sz, vp, vp, vp], C.c_int),
     "ngs_pcg_block_capacity": ([C.c_int], C.c_int),
     "ngs_pcg_blocks": ([i64, i64, C.c_int], C.c_int),
+    "ngs_pcg_window": ([i64, i64, i64, C.c_int], C.c_int),
     "ngs_pcg_cluster_size": ([i64, i64, C.c_int], C.c_int),
     "ngs_pcg_solve_batch": ([C.POINTER(PcgBatchItem), C.c_int, vp], C.c_int),
     "ngs_pcg_noalloc_max_rows": ([], i64),

@@ -479,7 +479,12 @@ class Reconstruction(DualMesher):
             if lv.mf:
                 self._assemble_mf(lv, d)
             if not lv.mf or self.keep_csr:
-                self._assemble_csr(lv, d, bool(span[d] <= 32767))
+                # 2-byte column deltas where every |column - row| fits and the solver reads them
+                # (the launches that stage the vector in shared memory)
+                mode = self.solver.mode
+                delta_ok = bool(span[d] <= 32767 and mode is not None and
+                                L.load().ngs_pcg_window(lv.n, lv.nnz, lv.band, mode) == 1)
+                self._assemble_csr(lv, d, delta_ok)
         self._mark("assembly")
         return self
 

@@ -3,11 +3,12 @@
 A system whose ``band`` (bound on |column - row|) lets every block's column range fit stages the
 search vector in shared memory; with ``band = 0`` the launch reserves none and the gathers read
 global memory.  The window changes only where the same values are read, so the two solutions are
-bit-identical.  2-byte column deltas take the software-pipelined SpMV (four entries per round),
-4-byte columns the row-at-a-time one (eight per round): their products round differently, and both
-converge to the same solution within the solve tolerance.  Systems: 7-point Laplacians plus a shift
-(sorted columns within every row), one solved by a thread-block cluster and one by a cooperative
-grid.
+bit-identical.  With the window the solver reads the 2-byte column deltas, if given, in the
+software-pipelined SpMV (four entries per round); without it, the 4-byte columns in the
+row-at-a-time one (eight per round) -- given deltas are then ignored, which this also checks bit for
+bit.  The two forms' products round differently, and both converge to the same solution within the
+solve tolerance.  Systems: 7-point Laplacians plus a shift (sorted columns within every row), one
+solved by a thread-block cluster and one by a cooperative grid.
 """
 import ctypes as C
 
@@ -63,14 +64,16 @@ def test_window_changes_no_bit_and_both_spmv_forms_converge(side):
     gen = torch.Generator(device="cpu").manual_seed(side)
     b = torch.randn(m["n"], generator=gen, dtype=torch.float64).to(DEV)
     band = side * side                      # the +-x neighbours are the farthest columns
-    for deltas in (False, True):
-        x_glob, it_glob = solve(m, b, 0, deltas)
-        x_win, it_win = solve(m, b, band, deltas)
-        assert it_glob == it_win
-        assert torch.equal(x_glob, x_win), "the window must not change a bit"
-    x32cols, _ = solve(m, b, band, False)
-    x16cols, _ = solve(m, b, band, True)
-    rel = float(torch.linalg.norm(x32cols - x16cols) / torch.linalg.norm(x32cols))
+    assert lib.ngs_pcg_window(m["n"], m["nnz"], band, L.PCG_MIXED) == 1
+    assert lib.ngs_pcg_window(m["n"], m["nnz"], 0, L.PCG_MIXED) == 0
+    x_glob, it_glob = solve(m, b, 0, False)
+    x_win, it_win = solve(m, b, band, False)
+    assert it_glob == it_win
+    assert torch.equal(x_glob, x_win), "the window must not change a bit"
+    x_glob_d, _ = solve(m, b, 0, True)      # no window: the deltas are not read
+    assert torch.equal(x_glob, x_glob_d)
+    x_win_d, _ = solve(m, b, band, True)    # window: the deltas, the pipelined form
+    rel = float(torch.linalg.norm(x_win - x_win_d) / torch.linalg.norm(x_win))
     # both solutions are within the solve tolerance of the exact one; the Laplacian's condition
     # number at these sizes (< 1e3 with the shift) bounds their distance well below 1e-6
     assert rel < 1e-6, rel
