@@ -767,6 +767,16 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_cluster_kerne
   cluster_sync_all();            // no CTA exits while another may still read its shared memory
 }
 
+// The cluster solve of an assembled matrix with its SpMV form fixed at compile time (the matrices
+// of cluster-sized systems are far below the streaming threshold: the unstreamed forms only).
+template <int MODE, int FORM>
+__global__ void __launch_bounds__(PCG_THREADS, PCG_MIN_BLOCKS) pcg_cluster_form_kernel(const __grid_constant__ PcgArgs a) {
+  __shared__ double cred[8], bcast[4];
+  ClusterSync sy{cluster_rank(), cluster_size(), cred, bcast, 0, 0ull, a.budget_ns, false};
+  pcg_body<MODE, PCG_OPS_CSR, FORM>(a, sy.rank, sy);
+  cluster_sync_all();
+}
+
 // A batch of independent systems in one cooperative launch: system k owns the blocks
 // [start[k], start[k+1]), with the block count its single solve would use, so that its tile plan,
 // its reductions and therefore its result are bit-identical to solving it alone.  Every system has
@@ -899,8 +909,11 @@ static int pcg_cluster_limit() {
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && cached[dev] != 0) return cached[dev] > 0 ? cached[dev] : 0;
   int limit = pcg_cluster_limit_of_kernel((const void*)pcg_cluster_kernel<MODE, PCG_OPS_CSR>);
-  if constexpr (MODE != NGS_PCG_REFERENCE)
+  if constexpr (MODE != NGS_PCG_REFERENCE) {
     limit = std::min(limit, pcg_cluster_limit_of_kernel((const void*)pcg_cluster_kernel<MODE, PCG_OPS_MF>));
+    limit = std::min(limit, pcg_cluster_limit_of_kernel((const void*)pcg_cluster_form_kernel<MODE, PCG_FORM_DELTA>));
+    limit = std::min(limit, pcg_cluster_limit_of_kernel((const void*)pcg_cluster_form_kernel<MODE, PCG_FORM_COLS>));
+  }
   if (limit > PCG_CLUSTER_MAX) limit = PCG_CLUSTER_MAX;
   if (dev >= 0 && dev < 64) cached[dev] = limit > 0 ? limit : -1;
   return limit;
@@ -998,6 +1011,14 @@ static int launch_cluster(PcgArgs& a, int mode, int csize, cudaStream_t st) {
   void* args[] = {&a};
   ngs_count_launch();
   const void* f = pcg_cluster_kernel_of(mode, a.mf != 0);
+  if (!a.mf && !a.evict_first && (mode == NGS_PCG_MIXED || mode == NGS_PCG_FP64)) {
+    if (mode == NGS_PCG_MIXED)
+      f = a.cols16 ? (const void*)pcg_cluster_form_kernel<NGS_PCG_MIXED, PCG_FORM_DELTA>
+                   : (const void*)pcg_cluster_form_kernel<NGS_PCG_MIXED, PCG_FORM_COLS>;
+    else
+      f = a.cols16 ? (const void*)pcg_cluster_form_kernel<NGS_PCG_FP64, PCG_FORM_DELTA>
+                   : (const void*)pcg_cluster_form_kernel<NGS_PCG_FP64, PCG_FORM_COLS>;
+  }
   const cudaError_t e = cudaLaunchKernelExC(&lc, f, args);
   if (e != cudaSuccess) return ngs_set_cuda_error(e);
   return NGS_OK;
