@@ -11,11 +11,13 @@
 //     barrier + reduce     every block publishes its partials, arrives, and once all
 //                          have arrived sums all partials itself in block order
 //                          (deterministic, the same bits in every block).
-// The SpMV streams the CSR arrays straight from HBM: eight lanes per row, each lane
-// with up to eight (column, value) pairs and their vector gathers in flight per round, at
-// two blocks per SM.  (Staging CSR tiles through shared memory with bulk copies ran at
-// less than half this rate: the product and row-sum passes over shared memory, not
-// the copies, bounded it.)
+// The SpMV streams the CSR arrays straight from HBM: eight lanes per row at two blocks per SM,
+// in one of two forms -- 4-byte columns, a row at a time with up to eight (column, value) pairs
+// and their vector gathers in flight per lane, or 2-byte column deltas in a software-pipelined
+// loop that gathers from a shared-memory window of the vector -- each with its own kernel for the
+// single-system and cluster solves.  (Staging CSR tiles through shared memory with bulk copies ran
+// at less than half this rate: the product and row-sum passes over shared memory, not the copies,
+// bounded it.)
 // Every wait is bounded by the global nanosecond timer; on timeout the kernel
 // records NGS_ERR_TIMEOUT and returns.  Every solve is bounded too: at most
 // NGS_PCG_ITER_CAP iterations, and a deadline that block 0 checks at each
@@ -24,7 +26,7 @@
 //
 // Mixed precision (NGS_PCG_MIXED) is iterative refinement: the inner PCG runs on
 // the FP32 matrix with FP32 search vectors (SpMV products summed in FP32 over rounds
-// of eight, the rounds in FP64), FP64 dots, and FP64 x and r, until its residual
+// of four or eight, the rounds in FP64), FP64 dots, and FP64 x and r, until its residual
 // has dropped by `inner_rtol`; then
 // the true residual b - A x is formed with the FP64 matrix and the inner solve
 // restarts from it.  The FP32 matrix is a fixed SPD perturbation of the FP64 one,
@@ -32,8 +34,9 @@
 // solve converges to the FP64 system.
 //
 // This file is compiled without multiply-add contraction (build.py): the solver body is inlined
-// into the single-system and the batched kernel, and only uncontracted arithmetic is guaranteed to
-// round the same way in both, which makes a batched solve bit-identical to the solo one.
+// into the single-system, cluster and batched kernels, and only uncontracted arithmetic is
+// guaranteed to round the same way in all of them, which makes a batched solve bit-identical to
+// the solo one.
 #include <algorithm>
 #include <cmath>
 #include "mf.cuh"
