@@ -342,8 +342,8 @@ class Reconstruction(DualMesher):
         self.solve_hook = None     # callable(rec, level, d, item): hands the level's PCG to a batcher
         # largest dual-grid rank bitmap (16-byte words) before the mesh switches to sorted keys
         self.dual_grid_max_words = 1 << 27
-        # level operator of the solver: "csr" = the assembled matrix (the faster one on B200: its SpMV
-        # gathers from a shared-memory window of the vector); "matrix-free" = the stencil over the
+        # level operator of the solver: "csr" = the assembled matrix (the faster one on B200: one
+        # streamed pass over stored entries per product); "matrix-free" = the stencil over the
         # bitmap plus the point form of the screening, on the levels where the point pairs are fewer
         # than the stiffness non-zeros (FP32-mixed and FP64 solvers)
         if operator not in ("csr", "matrix-free"):
@@ -352,7 +352,8 @@ class Reconstruction(DualMesher):
         self.keep_csr = False      # also assemble the CSR of matrix-free levels (tests compare it)
         # longest pair list of a level whose screening terms go by rows from the transposed pairs (no
         # atomics, no sort); 0: every CSR level groups its points by cell (sort + FP64 atomics per cell
-        # chunk), which measured faster on the 300k benchmark (33.5 against 35.0 ms per reconstruction)
+        # chunk), which measured faster on the 300k benchmark (30.5 ms per reconstruction, against 33.0
+        # with the pair form on levels 0-2 and 49.0 on every level)
         self.pair_row_limit = 0
 
     def _mark(self, name):
