@@ -948,7 +948,7 @@ static void pcg_set_window(PcgArgs& a, int mode, int64_t band, int64_t nblocks);
 // Whether a solo solve of such a system stages its search vector in shared memory (the same decision
 // as ngs_pcg_solve), so that a caller builds 2-byte column deltas only where they are read.
 extern "C" int ngs_pcg_window(int64_t n, int64_t nnz, int64_t band, int mode) {
-  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0 || band <= 0) return 0;
+  if (mode < NGS_PCG_REFERENCE || mode > NGS_PCG_FP64 || n <= 0 || nnz < 0 || band <= 0) return 0;
   const int csize = ngs_pcg_cluster_size(n, nnz, mode);
   const int64_t blocks = csize > 0 ? csize : pcg_blocks_for(n, nnz, 0, capacity_of(mode));
   if (blocks < 1) return 0;
